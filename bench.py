@@ -1,0 +1,338 @@
+"""Benchmark: input MB/s of the matching path on B200.
+
+Workload (default): the Hamming k-mer set — 1000 random ACGT 25-mers with <= 3
+substitutions (166k STEs), a 16 MiB ACGT stream with mutated copies every
+64 KiB, cut into 16 segments of 1 MiB (the reference's throughput runs use
+1 MB segments), 10 groups, prefix depth 3, algorithm nonblockingallgroups.
+A step = one match of the whole stream + device sort/unique of the reports.
+
+  value  inputs already in HBM (16 MiB < L2, so L2 is flushed between steps)
+  e2e    through the public API with host buffers: pinned H2D of the stream,
+         match, D2H of the unique reports, every step
+Under torchrun each rank matches its own copy of the workload (independent
+segments, no data-path collective): weak scaling; value = all bytes / the
+slowest rank's time.
+
+`--impl reference` times the reference CPU matcher (the oracle's restatement
+of automataGroupsReference, code/src/ngap/ngap.cu:2171-2268) on a bounded
+sample of the same workload with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "input MB/s on 1 B200 (bit-exact reports)"
+SEG = 1 << 20
+
+
+def workload_args(name):
+    from ngap_b200 import workloads as W
+    if name == "hamming_set":
+        anml, data = W.hamming_set(seed=2)
+        return anml, data, dict(group_num=10, depth=3, seg_len=SEG, algorithm="nonblockingallgroups",
+                                desc="1000 ACGT 25-mers, Hamming <= 3 (166k STEs), 16 MiB, 16 x 1 MiB segments")
+    if name == "literal_set":
+        anml, data = W.literal_set(seed=1)
+        return anml, data, dict(group_num=1, depth=3, seg_len=len(data), algorithm="nonblockingallgroups",
+                                desc="64 literals 8-16 B with classes (786 STEs), 1 MiB single segment")
+    if name == "high_frontier":
+        anml, data = W.high_frontier(seed=3)
+        return anml, data, dict(group_num=10, depth=2, seg_len=SEG, algorithm="nonblockingallgroups",
+                                desc="500 Levenshtein-2 20-mers + 2000 lit.*lit, 32 MiB, 32 x 1 MiB segments")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(workload):
+    """DRAM bytes per launch of the matching kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "match_kernel_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(workload)
+    return None if v is None else float(v["dram_bytes_per_launch"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(stats, n_in, n_reports, table_bytes):
+    """Bytes of the worklist formulation (input + per matched state 24 B of
+    queue/CSR traffic + 8 B per successor tested + 8 B per report + tables)."""
+    return (n_in + stats["matched"] * 24 + stats["matched_deg"] * 8 + n_reports * 8 + table_bytes)
+
+
+def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
+    """Times the oracle (reference CPU matcher restated) on a bounded sample:
+    the first segments of the stream, all host threads over (group, segment)."""
+    from oracle import oracle
+    ncores = os.cpu_count() or 1
+    views = groups.views()
+    nseg_total = len(data) // seg_len
+    nseg = 1
+    t0 = time.time()
+    reps, st = oracle.match(views, data[:seg_len], 1, seg_len, mode=0, nthreads=ncores)
+    dt = time.time() - t0
+    # grow the sample to roughly seconds_hint of CPU work
+    while dt < seconds_hint / 4 and nseg * 2 <= nseg_total:
+        nseg *= 2
+        t0 = time.time()
+        reps, st = oracle.match(views, data[:nseg * seg_len], nseg, seg_len, mode=0, nthreads=ncores)
+        dt = time.time() - t0
+    units = len(views) * nseg
+    return {
+        "value": (nseg * seg_len) / dt / 1e6, "unit": "MB/s", "cores": min(ncores, units),
+        "kind": "port",
+        "sample": f"{nseg} of {nseg_total} segments ({nseg * seg_len} B), {units} (group, segment) "
+                  f"units, {dt:.1f} s",
+        "stats": st, "sample_bytes": nseg * seg_len, "sample_reports": int(len(reps)),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hamming_set")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--check", action="store_true", help="verify the reports against the oracle")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import ngap_b200 as nb
+        anml, data, cfg = workload_args(args.workload)
+        groups = nb.Groups(nb.Nfa.from_string(anml), group_num=cfg["group_num"])
+        vals = []
+        for _ in range(warmup):
+            pass
+        per = max(5.0, 60.0 / max(1, args.steps))
+        for _ in range(args.steps):
+            cb = cpu_baseline(groups, data, cfg["seg_len"], seconds_hint=per)
+            vals.append(cb["value"])
+        v = float(np.mean(vals))
+        line = {"metric": METRIC, "value": v, "unit": "MB/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": args.workload, "desc": cfg["desc"],
+                           "group_num": cfg["group_num"], "seg_len": cfg["seg_len"]},
+                "cpu_baseline": {"value": v, "unit": "MB/s", "cores": cb["cores"], "kind": "port",
+                                 "sample": cb["sample"]},
+                "e2e": {"value": v, "unit": "MB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import ngap_b200 as nb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    anml, data, cfg = workload_args(args.workload)
+    nfa = nb.Nfa.from_string(anml)
+    groups = nb.Groups(nfa, group_num=cfg["group_num"])
+    tables = nb.Tables(groups, device=local_rank, precompute_depth=cfg["depth"])
+    eng = nb.Engine(local_rank)
+    seg_len = cfg["seg_len"]
+    num_seg = len(data) // seg_len
+    n_in = num_seg * seg_len
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    d_in = torch.from_numpy(data[:n_in]).to(f"cuda:{local_rank}")
+    h_pinned = torch.from_numpy(data[:n_in].copy()).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    kw = dict(algorithm=cfg["algorithm"], stream=sh)
+
+    def step_device():
+        eng.match_async(tables, d_in, num_seg, seg_len, **kw)
+
+    # warm-up (also validates)
+    for _ in range(warmup):
+        step_device()
+        eng.sync()
+    raw, uniq = eng.counts()
+    check = None
+    if args.check:
+        from oracle import oracle
+        want, _ = oracle.match(groups.views(), data[:n_in], num_seg, seg_len)
+        check = bool(np.array_equal(eng.results(), want))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    match_ms, launches = [], 0
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()  # evict the 16 MiB stream from L2 (outside the step's events)
+            evs[i][0].record(stream)
+            step_device()
+            evs[i][1].record(stream)
+            eng.sync()
+            match_ms.append(eng.times_ms()[0])
+            launches += eng.launches()
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    t_ms = float(sum(step_ms))
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * n_in * args.steps / (t_ms / 1e3) / 1e6
+
+    # ---- end to end through the public API with host buffers
+    e2e_ms = []
+    d2h = 0
+    barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.match_async(tables, h_pinned.numpy(), num_seg, seg_len, **kw)
+        eng.sync()
+        res = eng.results()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+        d2h = res.nbytes + 40
+    e2e_total = float(sum(e2e_ms))
+    if dist is not None:
+        tt = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = world * n_in * args.steps / (e2e_total / 1e3) / 1e6
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        line = {"metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded generator, same shapes as the benchmark config)",
+                "config": {"workload": args.workload, "desc": cfg["desc"],
+                           "algorithm": cfg["algorithm"], "group_num": groups.count,
+                           "precompute_depth": cfg["depth"], "num_seg": num_seg, "seg_len": seg_len,
+                           "input_bytes": n_in, "l2": "flushed between steps (256 MiB write)"},
+                "reports": {"raw": raw, "unique": uniq},
+                "gpu_launches": launches,
+                "clocks": clk.summary(),
+                "e2e": {"value": e2e_value, "unit": "MB/s", "h2d_bytes_per_step": n_in,
+                        "d2h_bytes_per_step": d2h},
+                }
+        if check is not None:
+            line["parity_vs_oracle"] = check
+        mk = float(np.mean(match_ms))
+        roof = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                "kernel": "match_kernel", "kernel_ms": mk}
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(groups, data[:n_in], seg_len)
+            st = cb.pop("stats")
+            scale = n_in / cb.pop("sample_bytes")
+            cb.pop("sample_reports")
+            stats_full = {k: v * scale for k, v in st.items()}
+            alg = algorithmic_bytes(stats_full, n_in, uniq, tables.device_bytes)
+            roof.update({"achieved": alg / (mk / 1e3) / 1e9, "algorithmic_bytes": alg,
+                         "bytes_per_input_byte": alg / n_in})
+            roof["frac"] = roof["achieved"] / peak
+            line["cpu_baseline"] = cb
+        tr = profiled_traffic(args.workload)
+        roof["traffic"] = tr
+        line["roofline"] = roof
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

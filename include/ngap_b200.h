@@ -1,0 +1,184 @@
+/*
+ * ngap_b200 — C ABI of the B200 automata-processing engine.
+ *
+ * The reference (getianao/ngAP) has no FFI; its in-process boundary is
+ * `class ngap` (code/src/ngap/ngap.h:27-177) driven by the CLI
+ * (code/src/ngap/main.cu:16-137). Each entry point below replaces one step of
+ * that flow; the reference interface it replaces is cited beside it.
+ *
+ * Conventions: every function returns an int status (NGAP_OK = 0) unless
+ * stated; ngap_last_error() gives the calling thread's last message. Nothing
+ * here calls exit(). Objects are not shared between host threads; the CUDA
+ * stream is passed explicitly. Report encoding is the reference's
+ * (ngap.cu:1899-1905): ((uint64)(sid | group << 22) << 32) | input_offset,
+ * sorted by (offset, id) and deduplicated (ngap.cu:19-30, 1928-1932).
+ */
+#ifndef NGAP_B200_H_
+#define NGAP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define NGAP_OK 0
+#define NGAP_E_INVALID 1          /* bad argument */
+#define NGAP_E_PARSE 2            /* ANML malformed or uses an unsupported element */
+#define NGAP_E_UNSUPPORTED 3      /* unsupported file type or size */
+#define NGAP_E_DEGREE 4           /* a CC's out-degree could not be limited (quit requested) */
+#define NGAP_E_CUDA 5             /* CUDA runtime error (message has details) */
+#define NGAP_E_OVERFLOW_QUEUE 6   /* a worklist exceeded its capacity; results incomplete */
+#define NGAP_E_OVERFLOW_RESULTS 7 /* more reports than result_capacity; results truncated */
+#define NGAP_E_TIMEOUT 8          /* a bounded device wait gave up */
+#define NGAP_E_NOMEM 9            /* allocation failed */
+#define NGAP_E_IO 10              /* file could not be read */
+
+/* ---- algorithms (the --algorithm values, code/src/ngap/main.cu:114-130) ---- */
+#define NGAP_ALGO_BLOCKING 0        /* blockinggroups      (BAP, kernel_ngap_O0.cu) */
+#define NGAP_ALGO_NAP 1             /* NAPgroups           (kernel_bap.cu) */
+#define NGAP_ALGO_NONBLOCKING 2     /* nonblockinggroups   (O1, kernel_ngap_O1.cu) */
+#define NGAP_ALGO_NONBLOCKING_R1 3  /* nonblockingr1groups (kernel_ngap_O4.cu:7) */
+#define NGAP_ALGO_NONBLOCKING_R2 4  /* nonblockingr2groups (kernel_ngap_O4.cu:240) */
+#define NGAP_ALGO_NONBLOCKING_PC 5  /* nonblockingpcgroups (O1+O2, kernel_ngap_O3.cu) */
+#define NGAP_ALGO_NONBLOCKING_ALL 6 /* nonblockingallgroups (O1+O2+O3, kernel_ngap_OA.cu) */
+
+typedef struct ngap_nfa ngap_nfa;       /* parsed ANML */
+typedef struct ngap_groups ngap_groups; /* group graphs after preprocessing */
+typedef struct ngap_tables ngap_tables; /* device-resident matching tables */
+typedef struct ngap_engine ngap_engine; /* device buffers, results, timing */
+
+/* ---- front-end ---- */
+
+/* Replaces load_nfa_from_file / load_nfa_from_anml (code/src/commons/NFALoader.cpp:70-171). */
+int ngap_nfa_load_anml(const char* path, ngap_nfa** out);
+/* Same, from an in-memory ANML document. */
+int ngap_nfa_parse_anml(const char* xml, size_t len, ngap_nfa** out);
+void ngap_nfa_destroy(ngap_nfa* nfa);
+/* Counts of NFA::size / NFA::edge_size (code/src/commons/NFA.cpp:411-417). */
+int64_t ngap_nfa_num_states(const ngap_nfa* nfa);
+int64_t ngap_nfa_num_edges(const ngap_nfa* nfa);
+
+typedef struct ngap_group_opts {
+  int group_num;     /* --group-num (reference default 10) */
+  int max_nfa_size;  /* --max-nfa-size, -1 = no limit */
+  int quit_degree;   /* --quit-degree (default 1) */
+  int remove_degree; /* --remove-degree (default 0) */
+} ngap_group_opts;
+
+/* Replaces ngap::preprocessing (code/src/ngap/ngap.cu:63-91) followed by
+ * nfa_utils::group_nfas_by_num (code/src/commons/nfa_utils.cpp:382-424) and
+ * Graph::ReadNFA per group (code/src/commons/graph.cu:169-206). */
+int ngap_groups_build(const ngap_nfa* nfa, const ngap_group_opts* opts, ngap_groups** out);
+int ngap_groups_count(const ngap_groups* g);
+/* CCs before limiting, CCs dropped by the degree limiter, CCs dropped by size. */
+int ngap_groups_cc_stats(const ngap_groups* g, int64_t* total, int64_t* failed, int64_t* too_big);
+
+/* Host view of one group graph; pointers stay valid until ngap_groups_destroy. */
+typedef struct ngap_group_view {
+  int32_t num_states;
+  int32_t num_edges;
+  int32_t num_aas;
+  int32_t num_start;
+  int32_t num_ccs;
+  const int32_t* row_offsets;  /* [num_states + 1] */
+  const int32_t* col_indices;  /* [num_edges], sorted by (src, dst) */
+  const uint32_t* symbol_sets; /* [num_states * 8], bit s of word s/32 */
+  const uint8_t* node_attrs;   /* bit0 always-active, bit1 report */
+  const int32_t* always_active;/* [num_aas], ascending */
+  const int32_t* start_states; /* [num_start], start-of-data, ascending */
+  const int32_t* cc_begin;     /* [num_ccs + 1], first state of each CC */
+  const int32_t* orig_node;    /* [num_states], index of the ANML STE each state came from */
+} ngap_group_view;
+int ngap_group_view_get(const ngap_groups* g, int group, ngap_group_view* out);
+void ngap_groups_destroy(ngap_groups* g);
+
+/* ---- device tables ---- */
+
+typedef struct ngap_table_opts {
+  int device;            /* CUDA device ordinal */
+  int precompute_depth;  /* --precompute-depth 0..3: prefix-memoization depth */
+  int precompute_cutoff; /* --precompute-cutoff, -1 = mean list length (precompute_table.cu:171) */
+  int tile_states;       /* max states per tile; 0 = automatic */
+  int64_t max_table_entries; /* cap on prefix-table list entries per tile; 0 = automatic */
+} ngap_table_opts;
+
+/* Replaces GroupCsr/GroupMatchset/GroupNodeAttrs/GroupAAS::init
+ * (code/include/commons/group_graph.h:6-109) and ngap::initGroupCsrWithPrec
+ * (code/src/ngap/ngap.cu:3086-3111, prefix tables ngap.cu:2358-2513). */
+int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_tables** out);
+void ngap_tables_destroy(ngap_tables* t);
+/* Bytes of device memory held by the tables. */
+int64_t ngap_tables_device_bytes(const ngap_tables* t);
+
+/* ---- engine ---- */
+
+/* Replaces NonBlockingBuffer/BlockingBuffer allocation (code/src/ngap/ngap_buffer.cu:111-748). */
+int ngap_engine_create(int device, ngap_engine** out);
+void ngap_engine_destroy(ngap_engine* e);
+
+typedef struct ngap_match_params {
+  int algorithm;             /* NGAP_ALGO_* */
+  int64_t num_seg;           /* input segments (main.cu:88-102) */
+  int64_t seg_len;           /* bytes per segment; input holds num_seg * seg_len bytes */
+  int is_dup;                /* start-of-data states in every segment (ngap_buffer.cu:479-484) */
+  int unique;                /* --unique: drop duplicate worklist entries within a step */
+  int active_threshold;      /* --active-threshold: busy-lane count enabling privatization */
+  int report_off;            /* --report-off: count reports only */
+  uint64_t result_capacity;  /* --result-capacity */
+  int window;                /* positions per worklist window; 0 = automatic */
+  int chunk;                 /* positions per chunk of a bounded tile; 0 = automatic */
+} ngap_match_params;
+
+/* Replaces ngap::launch_*_groups (code/src/ngap/ngap.cu:115-2078) up to the
+ * report copy: matches `input` (host or device memory, num_seg * seg_len
+ * bytes) against every group and leaves the sorted, deduplicated reports on
+ * the device. Asynchronous on `stream` (a cudaStream_t, NULL = default);
+ * ngap_engine_sync waits and returns the run's status. */
+int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int input_on_device,
+               const ngap_match_params* p, void* stream);
+int ngap_engine_sync(ngap_engine* e);
+
+/* Results of the last ngap_match (after ngap_engine_sync). raw = reports
+ * emitted by the kernel (duplicates included), unique = after sort+unique. */
+int ngap_results_count(const ngap_engine* e, uint64_t* raw, uint64_t* unique);
+/* Device pointer to the unique reports (valid until the next match). */
+const uint64_t* ngap_results_device(const ngap_engine* e);
+/* Copies up to cap unique reports to host memory; returns how many were copied. */
+int64_t ngap_results_copy(ngap_engine* e, uint64_t* host, uint64_t cap);
+/* Device time of the last match in milliseconds: [0] matching kernel, [1] sort+unique. */
+int ngap_last_times_ms(const ngap_engine* e, float* match_ms, float* sort_ms);
+/* Kernel launches issued by the last ngap_match. */
+int ngap_last_launches(const ngap_engine* e);
+/* Worklist entries expanded and always-active entries injected by the last match. */
+int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injected);
+
+/* ---- report compaction ---- */
+
+/* Sorts n packed reports (reference encoding) in device memory by (offset, id)
+ * with the engine's radix sort and removes duplicates; writes the result to
+ * d_out (may alias nothing) and its length to *n_out (host). */
+int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                             uint64_t* n_out, void* stream);
+
+/* ---- CPU checker used by the CLI's --validation (ngap.cu:2171-2344) ---- */
+
+/* Runs the reference's CPU frontier simulation over the group graphs and
+ * writes the sorted, deduplicated reports; returns the count or -1 if more
+ * than cap. This is a checker for the CLI's --validation flag only: it never
+ * produces the engine's results. */
+int64_t ngap_cpu_validate_reference(const ngap_groups* g, const uint8_t* input, int64_t num_seg,
+                                    int64_t seg_len, int is_dup, uint64_t* out, int64_t cap,
+                                    double* elapsed_ms);
+
+/* Message of the calling thread's last error. Returns its length. */
+int ngap_last_error(char* buf, size_t n);
+/* Library version string. */
+const char* ngap_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NGAP_B200_H_ */

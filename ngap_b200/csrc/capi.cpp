@@ -1,0 +1,203 @@
+// Host-side C ABI: errors, ANML front-end, grouping, group views and the
+// CPU checker behind the CLI's --validation flag.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <thread>
+
+#include "common.h"
+#include "handles.h"
+
+namespace ngap {
+
+namespace {
+thread_local std::string g_err;
+}
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+const std::string& last_error() { return g_err; }
+
+}  // namespace ngap
+
+using namespace ngap;
+
+extern "C" {
+
+int ngap_last_error(char* buf, size_t n) {
+  const std::string& e = last_error();
+  if (buf && n > 0) {
+    size_t k = std::min(n - 1, e.size());
+    memcpy(buf, e.data(), k);
+    buf[k] = '\0';
+  }
+  return (int)e.size();
+}
+
+const char* ngap_version(void) { return "ngap_b200 0.1.0 (sm_100a)"; }
+
+int ngap_nfa_load_anml(const char* path, ngap_nfa** out) {
+  if (!path || !out) {
+    set_error("ngap_nfa_load_anml: null argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  std::unique_ptr<ngap_nfa> h(new ngap_nfa());
+  int rc = load_anml_file(path, h->nfa);
+  if (rc != NGAP_OK) return rc;
+  *out = h.release();
+  return NGAP_OK;
+}
+
+int ngap_nfa_parse_anml(const char* xml, size_t len, ngap_nfa** out) {
+  if (!xml || !out) {
+    set_error("ngap_nfa_parse_anml: null argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  std::unique_ptr<ngap_nfa> h(new ngap_nfa());
+  int rc = parse_anml(xml, len, h->nfa);
+  if (rc != NGAP_OK) return rc;
+  *out = h.release();
+  return NGAP_OK;
+}
+
+void ngap_nfa_destroy(ngap_nfa* nfa) { delete nfa; }
+
+int64_t ngap_nfa_num_states(const ngap_nfa* nfa) { return nfa ? (int64_t)nfa->nfa.nodes.size() : -1; }
+
+int64_t ngap_nfa_num_edges(const ngap_nfa* nfa) { return nfa ? nfa->nfa.num_edges() : -1; }
+
+int ngap_groups_build(const ngap_nfa* nfa, const ngap_group_opts* opts, ngap_groups** out) {
+  if (!nfa || !out) {
+    set_error("ngap_groups_build: null argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  GroupOpts o;
+  if (opts) {
+    o.group_num = opts->group_num;
+    o.max_nfa_size = opts->max_nfa_size;
+    o.quit_degree = opts->quit_degree != 0;
+    o.remove_degree = opts->remove_degree != 0;
+  }
+  std::unique_ptr<ngap_groups> h(new ngap_groups());
+  int rc = build_groups(nfa->nfa, o, h->gs);
+  if (rc != NGAP_OK) return rc;
+  *out = h.release();
+  return NGAP_OK;
+}
+
+int ngap_groups_count(const ngap_groups* g) { return g ? (int)g->gs.groups.size() : -1; }
+
+int ngap_groups_cc_stats(const ngap_groups* g, int64_t* total, int64_t* failed, int64_t* too_big) {
+  if (!g) return NGAP_E_INVALID;
+  if (total) *total = g->gs.num_ccs_total;
+  if (failed) *failed = g->gs.num_ccs_failed;
+  if (too_big) *too_big = g->gs.num_ccs_too_big;
+  return NGAP_OK;
+}
+
+int ngap_group_view_get(const ngap_groups* g, int group, ngap_group_view* out) {
+  if (!g || !out || group < 0 || group >= (int)g->gs.groups.size()) {
+    set_error("ngap_group_view_get: bad argument");
+    return NGAP_E_INVALID;
+  }
+  const GroupGraph& gg = g->gs.groups[group];
+  out->num_states = gg.V;
+  out->num_edges = gg.E;
+  out->num_aas = (int32_t)gg.aas.size();
+  out->num_start = (int32_t)gg.starts.size();
+  out->num_ccs = (int32_t)gg.cc_begin.size() - 1;
+  out->row_offsets = gg.row_offsets.data();
+  out->col_indices = gg.cols.data();
+  out->symbol_sets = gg.bits.data();
+  out->node_attrs = gg.attrs.data();
+  out->always_active = gg.aas.data();
+  out->start_states = gg.starts.data();
+  out->cc_begin = gg.cc_begin.data();
+  out->orig_node = gg.orig_node.data();
+  return NGAP_OK;
+}
+
+void ngap_groups_destroy(ngap_groups* g) { delete g; }
+
+// The reference validates with a CPU frontier simulation (ngap.cu:2171-2268)
+// and a sort/unique comparison (ngap.cu:2270-2344). This checker does the same
+// with a deduplicated frontier; it is used by the CLI's --validation only.
+int64_t ngap_cpu_validate_reference(const ngap_groups* g, const uint8_t* input, int64_t num_seg,
+                                    int64_t seg_len, int is_dup, uint64_t* out, int64_t cap,
+                                    double* elapsed_ms) {
+  if (!g || (!input && num_seg * seg_len > 0)) return -1;
+  auto t0 = std::chrono::high_resolution_clock::now();
+  const int ngroups = (int)g->gs.groups.size();
+  const int64_t units = (int64_t)ngroups * num_seg;
+  std::vector<std::vector<uint64_t>> per(units);
+  unsigned nth = std::max(1u, std::thread::hardware_concurrency());
+  std::vector<std::thread> pool;
+  std::atomic<int64_t> next(0);
+  auto worker = [&]() {
+    std::vector<int32_t> cur, nxt;
+    std::vector<uint8_t> mark;
+    while (true) {
+      int64_t u = next.fetch_add(1);
+      if (u >= units) break;
+      const int gi = (int)(u / num_seg);
+      const int64_t seg = u % num_seg;
+      const GroupGraph& gg = g->gs.groups[gi];
+      mark.assign(gg.V, 0);
+      cur.clear();
+      if (seg == 0 || is_dup) cur.insert(cur.end(), gg.starts.begin(), gg.starts.end());
+      cur.insert(cur.end(), gg.aas.begin(), gg.aas.end());
+      std::sort(cur.begin(), cur.end());
+      cur.erase(std::unique(cur.begin(), cur.end()), cur.end());
+      const int64_t lo = seg * seg_len, hi = lo + seg_len;
+      std::vector<uint64_t>& rep = per[u];
+      for (int64_t it = lo; it < hi && !cur.empty(); it++) {
+        const uint8_t s = input[it];
+        nxt.clear();
+        for (int32_t v : cur) {
+          if (!((gg.bits[(size_t)v * 8 + (s >> 5)] >> (s & 31)) & 1u)) continue;
+          if (gg.attrs[v] & 2) rep.push_back(((uint64_t)it << 32) | ((uint32_t)v | ((uint32_t)gi << 22)));
+          for (int32_t e = gg.row_offsets[v]; e < gg.row_offsets[v + 1]; e++) {
+            int32_t x = gg.cols[e];
+            if (!mark[x]) {
+              mark[x] = 1;
+              nxt.push_back(x);
+            }
+          }
+        }
+        for (int32_t a : gg.aas)
+          if (!mark[a]) {
+            mark[a] = 1;
+            nxt.push_back(a);
+          }
+        for (int32_t x : nxt) mark[x] = 0;
+        cur.swap(nxt);
+      }
+    }
+  };
+  for (unsigned i = 0; i < nth; i++) pool.emplace_back(worker);
+  for (auto& th : pool) th.join();
+  std::vector<uint64_t> all;
+  for (auto& v : per) all.insert(all.end(), v.begin(), v.end());
+  std::sort(all.begin(), all.end());
+  all.erase(std::unique(all.begin(), all.end()), all.end());
+  auto t1 = std::chrono::high_resolution_clock::now();
+  if (elapsed_ms) *elapsed_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  if ((int64_t)all.size() > cap) return -1;
+  for (size_t i = 0; i < all.size(); i++) out[i] = (all[i] << 32) | (all[i] >> 32);
+  return (int64_t)all.size();
+}
+
+}  // extern "C"

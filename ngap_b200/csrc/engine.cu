@@ -1,0 +1,634 @@
+// Device side of the C ABI: table upload, work planning, kernel launches,
+// report compaction and results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+#include "common.h"
+#include "handles.h"
+#include "match_kernel.cuh"
+#include "sort_kernels.cuh"
+#include "tables.h"
+
+using namespace ngap;
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                     \
+  do {                                                                                     \
+    cudaError_t _e = (expr);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      set_error("CUDA error %s at %s:%d: %s", cudaGetErrorName(_e), __FILE__, __LINE__,    \
+                cudaGetErrorString(_e));                                                   \
+      return NGAP_E_CUDA;                                                                  \
+    }                                                                                      \
+  } while (0)
+
+int bits_for(uint64_t x) {  // bits needed to hold values < x (x >= 1)
+  int b = 0;
+  while (b < 64 && (x - 1) >> b) b++;
+  return b;
+}
+
+}  // namespace
+
+struct ngap_tables {
+  int device = 0;
+  int num_groups = 0;
+  std::vector<TileHost> tiles;
+  std::vector<TileDev> dev_desc;
+  TileDev* d_tiles = nullptr;
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  int32_t max_states = 0;
+
+  ~ngap_tables() {
+    for (void* p : allocs) cudaFree(p);
+  }
+  template <class T>
+  int upload(const std::vector<T>& v, const T** out) {
+    *out = nullptr;
+    if (v.empty()) return NGAP_OK;
+    void* p = nullptr;
+    size_t b = v.size() * sizeof(T);
+    CUDA_TRY(cudaMalloc(&p, b));
+    allocs.push_back(p);
+    bytes += (int64_t)b;
+    CUDA_TRY(cudaMemcpy(p, v.data(), b, cudaMemcpyHostToDevice));
+    *out = static_cast<const T*>(p);
+    return NGAP_OK;
+  }
+};
+
+struct UnitPlanKey {
+  int64_t num_seg, seg_len;
+  int is_dup, window, chunk;
+  bool operator<(const UnitPlanKey& o) const {
+    return std::tie(num_seg, seg_len, is_dup, window, chunk) <
+           std::tie(o.num_seg, o.seg_len, o.is_dup, o.window, o.chunk);
+  }
+};
+
+struct ngap_engine {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  // input
+  uint8_t* d_input = nullptr;
+  size_t input_cap = 0;
+  // units (cached plan for one tables object)
+  const ngap_tables* plan_tables = nullptr;
+  UnitPlanKey plan_key{-1, -1, -1, -1, -1};
+  UnitDev* d_units = nullptr;
+  size_t units_cap = 0;
+  int32_t nunits = 0;
+  // reports
+  uint64_t rep_cap = 0;
+  uint64_t* d_reports = nullptr;
+  uint64_t* d_tmp = nullptr;
+  uint64_t* d_unique = nullptr;
+  uint32_t* d_hist = nullptr;
+  size_t hist_cap = 0;
+  // counters: [0] raw reports, [1] unique reports, [2] expanded, [3] injected
+  unsigned long long* d_counters = nullptr;
+  int* d_err = nullptr;
+  unsigned int* d_unit_counter = nullptr;
+  unsigned long long* h_counters = nullptr;  // pinned mirror (4 counters + err)
+  // per-warp scratch
+  uint32_t* d_carry = nullptr;
+  uint32_t* d_marks = nullptr;
+  uint32_t* d_ovf = nullptr;
+  size_t slots = 0;
+  int carry_cap = 0, mark_words = 0, ovf_cap = 0;
+  int max_smem_set = -1;
+  // timing
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float match_ms = 0.f, sort_ms = 0.f;
+  int launches = 0;
+  int pending_status = NGAP_OK;
+  bool ran = false;
+  int grid = 0;
+
+  ~ngap_engine() {
+    cudaFree(d_input);
+    cudaFree(d_units);
+    cudaFree(d_reports);
+    cudaFree(d_tmp);
+    cudaFree(d_unique);
+    cudaFree(d_hist);
+    cudaFree(d_counters);
+    cudaFree(d_err);
+    cudaFree(d_unit_counter);
+    cudaFree(d_carry);
+    cudaFree(d_marks);
+    cudaFree(d_ovf);
+    if (h_counters) cudaFreeHost(h_counters);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+extern "C" {
+
+int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_tables** out) {
+  if (!g || !out) {
+    set_error("ngap_tables_build: null argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  ngap_table_opts o{};
+  o.precompute_cutoff = -1;
+  if (opts) o = *opts;
+  if (o.precompute_depth < 0 || o.precompute_depth > kMaxDepth) {
+    set_error("precompute_depth must be in 0..%d (got %d)", kMaxDepth, o.precompute_depth);
+    return NGAP_E_INVALID;
+  }
+  std::unique_ptr<ngap_tables> t(new ngap_tables());
+  t->device = o.device;
+  CUDA_TRY(cudaSetDevice(o.device));
+  TableOpts to;
+  to.precompute_depth = o.precompute_depth;
+  to.precompute_cutoff = o.precompute_cutoff;
+  to.tile_states = o.tile_states;
+  to.max_table_entries = o.max_table_entries;
+  int rc = build_tiles(g->gs, to, t->tiles);
+  if (rc != NGAP_OK) return rc;
+  t->num_groups = (int)g->gs.groups.size();
+  for (auto& th : t->tiles) {
+    if (th.nstates >= kMaxTileStates - 1) {
+      set_error("a connected component has %d states; at most %d are supported per tile",
+                th.nstates, kMaxTileStates - 2);
+      return NGAP_E_UNSUPPORTED;
+    }
+    t->max_states = std::max(t->max_states, th.nstates);
+    TileDev d;
+    d.group = th.group;
+    d.nstates = th.nstates;
+    d.naas = (int32_t)th.aas.size();
+    d.nstart = (int32_t)th.start.size();
+    d.depth = th.depth;
+    d.max_path = th.max_path;
+    const uint32_t* succ = nullptr;
+    if ((rc = t->upload(th.succ, &succ)) != NGAP_OK) return rc;
+    d.succ = reinterpret_cast<const uint4*>(succ);
+    if ((rc = t->upload(th.bits, &d.bits)) != NGAP_OK) return rc;
+    if ((rc = t->upload(th.rep, &d.rep)) != NGAP_OK) return rc;
+    if ((rc = t->upload(th.sid, &d.sid)) != NGAP_OK) return rc;
+    if ((rc = t->upload(th.aas, &d.aas)) != NGAP_OK) return rc;
+    if ((rc = t->upload(th.start, &d.start)) != NGAP_OK) return rc;
+    for (int k = 0; k < kMaxDepth; k++) {
+      const PrefixTableHost& ph = th.pt[k];
+      PrefixTableDev& pd = d.pt[k];
+      pd.dense = ph.dense ? 1 : 0;
+      pd.nkeys = (int32_t)ph.keys.size();
+      pd.nrkeys = (int32_t)ph.rkeys.size();
+      pd.cutoff = ph.cutoff;
+      if ((rc = t->upload(ph.keys, &pd.keys)) != NGAP_OK) return rc;
+      if ((rc = t->upload(ph.voff, &pd.voff)) != NGAP_OK) return rc;
+      if ((rc = t->upload(ph.vlist, &pd.vlist)) != NGAP_OK) return rc;
+      if ((rc = t->upload(ph.rkeys, &pd.rkeys)) != NGAP_OK) return rc;
+      if ((rc = t->upload(ph.roff, &pd.roff)) != NGAP_OK) return rc;
+      if ((rc = t->upload(ph.rlist, &pd.rlist)) != NGAP_OK) return rc;
+    }
+    t->dev_desc.push_back(d);
+  }
+  const TileDev* dt = nullptr;
+  if ((rc = t->upload(t->dev_desc, &dt)) != NGAP_OK) return rc;
+  t->d_tiles = const_cast<TileDev*>(dt);
+  *out = t.release();
+  return NGAP_OK;
+}
+
+void ngap_tables_destroy(ngap_tables* t) { delete t; }
+
+int64_t ngap_tables_device_bytes(const ngap_tables* t) { return t ? t->bytes : 0; }
+
+int ngap_engine_create(int device, ngap_engine** out) {
+  if (!out) {
+    set_error("ngap_engine_create: null argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) {
+    set_error("no CUDA device %d (%d present)", device, ndev);
+    return NGAP_E_CUDA;
+  }
+  CUDA_TRY(cudaSetDevice(device));
+  std::unique_ptr<ngap_engine> e(new ngap_engine());
+  e->device = device;
+  CUDA_TRY(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaMalloc(&e->d_counters, 8 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMalloc(&e->d_err, sizeof(int)));
+  CUDA_TRY(cudaMalloc(&e->d_unit_counter, sizeof(unsigned int)));
+  CUDA_TRY(cudaMallocHost(&e->h_counters, 8 * sizeof(unsigned long long)));
+  for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
+  *out = e.release();
+  return NGAP_OK;
+}
+
+void ngap_engine_destroy(ngap_engine* e) {
+  if (e) {
+    cudaSetDevice(e->device);
+    delete e;
+  }
+}
+
+}  // extern "C"
+
+namespace {
+
+int ensure_reports(ngap_engine* e, uint64_t cap) {
+  if (cap <= e->rep_cap) return NGAP_OK;
+  cudaFree(e->d_reports);
+  cudaFree(e->d_tmp);
+  cudaFree(e->d_unique);
+  cudaFree(e->d_hist);
+  e->d_reports = e->d_tmp = e->d_unique = nullptr;
+  e->d_hist = nullptr;
+  e->rep_cap = 0;
+  CUDA_TRY(cudaMalloc(&e->d_reports, cap * sizeof(uint64_t)));
+  CUDA_TRY(cudaMalloc(&e->d_tmp, cap * sizeof(uint64_t)));
+  CUDA_TRY(cudaMalloc(&e->d_unique, cap * sizeof(uint64_t)));
+  size_t ntiles = (cap + kSortTile - 1) / kSortTile;
+  e->hist_cap = 16 * ntiles + 16;
+  CUDA_TRY(cudaMalloc(&e->d_hist, e->hist_cap * sizeof(uint32_t)));
+  e->rep_cap = cap;
+  return NGAP_OK;
+}
+
+int ensure_slots(ngap_engine* e, size_t slots, int max_states) {
+  int carry_cap = std::max(max_states, 32);
+  int mark_words = (max_states + 31) / 32 + 1;
+  int ovf_cap = 1 << 16;
+  if (slots <= e->slots && carry_cap <= e->carry_cap && mark_words <= e->mark_words) return NGAP_OK;
+  cudaFree(e->d_carry);
+  cudaFree(e->d_marks);
+  cudaFree(e->d_ovf);
+  e->d_carry = e->d_marks = e->d_ovf = nullptr;
+  e->slots = 0;
+  slots = std::max(slots, e->slots);
+  CUDA_TRY(cudaMalloc(&e->d_carry, slots * (size_t)carry_cap * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&e->d_marks, slots * (size_t)mark_words * sizeof(uint32_t)));
+  CUDA_TRY(cudaMemset(e->d_marks, 0, slots * (size_t)mark_words * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&e->d_ovf, slots * (size_t)ovf_cap * sizeof(uint32_t)));
+  e->slots = slots;
+  e->carry_cap = carry_cap;
+  e->mark_words = mark_words;
+  e->ovf_cap = ovf_cap;
+  return NGAP_OK;
+}
+
+// Splits the work into units: unbounded tiles get one unit per segment;
+// bounded tiles are cut into chunks of `chunk` emitted positions, each with
+// max_path - 1 positions of warm-up (clamped at the segment start).
+void plan_units(const ngap_tables* t, const UnitPlanKey& k, std::vector<UnitDev>& units) {
+  units.clear();
+  std::vector<UnitDev> bounded;
+  for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
+    const TileHost& th = t->tiles[ti];
+    for (int64_t s = 0; s < k.num_seg; s++) {
+      const int64_t slo = s * k.seg_len, shi = slo + k.seg_len;
+      const bool starts = (s == 0 || k.is_dup) && !th.start.empty();
+      if (th.max_path < 0) {
+        UnitDev u;
+        u.tile = ti;
+        u.flags = starts ? 1u : 0u;
+        u.lo = slo;
+        u.hi = shi;
+        u.emit_lo = slo;
+        units.push_back(u);
+        continue;
+      }
+      const int64_t warm = th.max_path > 0 ? th.max_path - 1 : 0;
+      // chunk length is independent of the window (the blocking algorithm
+      // runs one-position windows); a chunk should span at least its warm-up
+      const int64_t base = std::max<int64_t>(k.window, 2048);
+      int64_t chunk = k.chunk > 0 ? k.chunk : std::max<int64_t>(base - warm, base / 2);
+      chunk = std::max<int64_t>(chunk, 1);
+      for (int64_t em = slo; em < shi; em += chunk) {
+        UnitDev u;
+        u.tile = ti;
+        u.lo = std::max(slo, em - warm);
+        u.hi = std::min(em + chunk, shi);
+        u.emit_lo = em;
+        u.flags = (starts && u.lo == slo) ? 1u : 0u;
+        bounded.push_back(u);
+      }
+    }
+  }
+  units.insert(units.end(), bounded.begin(), bounded.end());
+}
+
+__global__ void swap_halves(uint64_t* a, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t x = a[i];
+    a[i] = (x << 32) | (x >> 32);
+  }
+}
+
+int set_smem(ngap_engine* e, int smem) {
+  if (e->max_smem_set >= smem) return NGAP_OK;
+  cudaError_t ce = cudaFuncSetAttribute(match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(match_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(match_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (ce != cudaSuccess) {
+    set_error("shared memory request of %d bytes rejected: %s", smem, cudaGetErrorString(ce));
+    return NGAP_E_CUDA;
+  }
+  e->max_smem_set = smem;
+  return NGAP_OK;
+}
+
+template <int PRIV>
+int blocks_per_sm(int smem, int* out) {
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, match_kernel<PRIV>, kCtaThreads, smem));
+  if (*out < 1) {
+    set_error("the matching kernel does not fit on an SM with %d bytes of shared memory", smem);
+    return NGAP_E_CUDA;
+  }
+  return NGAP_OK;
+}
+
+template <int PRIV>
+int launch_match(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t st) {
+  match_kernel<PRIV><<<e->grid, kCtaThreads, smem, st>>>(mp);
+  CUDA_TRY(cudaGetLastError());
+  return NGAP_OK;
+}
+
+// Sorts d_in[0 .. *d_n) (clamped to cap) into d_out as unique reference-encoded
+// reports; *d_unique_n receives the count. off_bits / id_bits bound the key.
+int sort_unique(ngap_engine* e, uint64_t* d_in, const unsigned long long* d_n, uint64_t cap,
+                int off_bits, int id_bits, uint64_t* d_out, unsigned long long* d_unique_n,
+                cudaStream_t st) {
+  const uint32_t max_tiles = (uint32_t)((cap + kSortTile - 1) / kSortTile);
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, e->num_sms * 8));
+  std::vector<int> shifts;
+  for (int b = 0; b < id_bits; b += 4) shifts.push_back(b);
+  for (int b = 0; b < off_bits; b += 4) shifts.push_back(32 + b);
+  // ping-pong between d_in (an engine-owned buffer) and d_tmp
+  uint64_t* src = d_in;
+  uint64_t* dst = e->d_tmp;
+  for (int sh : shifts) {
+    radix_hist<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, sh, e->d_hist);
+    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 16, nullptr);
+    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, d_n, cap, sh, e->d_hist);
+    e->launches += 3;
+    std::swap(src, dst);
+  }
+  unique_count<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist);
+  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 1, d_unique_n);
+  unique_write<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist, d_out);
+  e->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  return NGAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int input_on_device,
+               const ngap_match_params* p, void* stream) {
+  if (!e || !t || !p || (!input && p->num_seg * p->seg_len > 0)) {
+    set_error("ngap_match: null argument");
+    return NGAP_E_INVALID;
+  }
+  if (p->num_seg <= 0 || p->seg_len <= 0) {
+    set_error("ngap_match: num_seg and seg_len must be positive");
+    return NGAP_E_INVALID;
+  }
+  const uint64_t total = (uint64_t)p->num_seg * (uint64_t)p->seg_len;
+  if (total >= (1ull << 32)) {
+    set_error("ngap_match: input of %llu bytes exceeds the 32-bit offsets of the report format",
+              (unsigned long long)total);
+    return NGAP_E_UNSUPPORTED;
+  }
+  if (t->num_groups > 1024) {
+    set_error("ngap_match: at most 1024 groups fit the 32-bit report id");
+    return NGAP_E_UNSUPPORTED;
+  }
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  e->stream = st;
+  e->launches = 0;
+  e->ran = false;
+  int algo = p->algorithm;
+  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 2048;
+  int table_depth = 0;
+  for (auto& th : t->tiles) table_depth = std::max(table_depth, th.depth);
+  switch (algo) {
+    case NGAP_ALGO_BLOCKING: depth = 0; window = 1; break;
+    case NGAP_ALGO_NAP: depth = 0; break;
+    case NGAP_ALGO_NONBLOCKING: depth = 1; break;
+    case NGAP_ALGO_NONBLOCKING_R1: depth = 1; priv = 1; break;
+    case NGAP_ALGO_NONBLOCKING_R2: depth = 1; priv = 2; break;
+    case NGAP_ALGO_NONBLOCKING_PC: depth = std::max(1, table_depth); break;
+    case NGAP_ALGO_NONBLOCKING_ALL: depth = std::max(1, table_depth); priv = 1; break;
+    default:
+      set_error("not supported algoritm %d", algo);
+      return NGAP_E_INVALID;
+  }
+  window = std::min(window, kMaxWindow);
+  // input: own 16-byte-aligned, padded copy
+  size_t need = ((total + 15) & ~(uint64_t)15) + 64;
+  if (need > e->input_cap) {
+    cudaFree(e->d_input);
+    e->d_input = nullptr;
+    e->input_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_input, need));
+    e->input_cap = need;
+  }
+  uint64_t cap = p->result_capacity > 0 ? p->result_capacity : 54619400ull;
+  int rc = ensure_reports(e, cap);
+  if (rc != NGAP_OK) return rc;
+  // units
+  UnitPlanKey key{p->num_seg, p->seg_len, p->is_dup ? 1 : 0, window, p->chunk};
+  if (e->plan_tables != t || key < e->plan_key || e->plan_key < key) {
+    std::vector<UnitDev> units;
+    plan_units(t, key, units);
+    if (units.size() > e->units_cap) {
+      cudaFree(e->d_units);
+      e->d_units = nullptr;
+      e->units_cap = 0;
+      CUDA_TRY(cudaMalloc(&e->d_units, units.size() * sizeof(UnitDev)));
+      e->units_cap = units.size();
+    }
+    if (!units.empty())
+      CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
+                          cudaMemcpyHostToDevice));
+    e->nunits = (int32_t)units.size();
+    e->plan_tables = t;
+    e->plan_key = key;
+  }
+  const int smem = kWarpsPerCta * warp_smem_bytes(window);
+  if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
+  int bps = 0;
+  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
+                                                              : blocks_per_sm<2>(smem, &bps);
+  if (rc != NGAP_OK) return rc;
+  int grid = e->num_sms * bps;
+  int need_blocks = (e->nunits + kWarpsPerCta - 1) / kWarpsPerCta;
+  grid = std::max(1, std::min(grid, need_blocks));
+  e->grid = grid;
+  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states);
+  if (rc != NGAP_OK) return rc;
+
+  CUDA_TRY(cudaEventRecord(e->ev[0], st));
+  if (input_on_device)
+    CUDA_TRY(cudaMemcpyAsync(e->d_input, input, total, cudaMemcpyDeviceToDevice, st));
+  else
+    CUDA_TRY(cudaMemcpyAsync(e->d_input, input, total, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(e->d_counters, 0, 8 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(e->d_err, 0, sizeof(int), st));
+  CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, sizeof(unsigned int), st));
+
+  MatchParams mp;
+  mp.tiles = t->d_tiles;
+  mp.units = e->d_units;
+  mp.nunits = e->nunits;
+  mp.input = e->d_input;
+  mp.window = window;
+  mp.depth = depth;
+  mp.active_threshold = p->active_threshold;
+  mp.unique = p->unique;
+  mp.report_off = p->report_off;
+  mp.rep_count = e->d_counters + 0;
+  mp.reports = e->d_reports;
+  mp.rep_cap = cap;
+  mp.err = e->d_err;
+  mp.unit_counter = e->d_unit_counter;
+  mp.carry = e->d_carry;
+  mp.marks = e->d_marks;
+  mp.ovf = e->d_ovf;
+  mp.carry_cap = e->carry_cap;
+  mp.mark_words = e->mark_words;
+  mp.ovf_cap = e->ovf_cap;
+  mp.work = e->d_counters + 2;
+  CUDA_TRY(cudaEventRecord(e->ev[1], st));
+  if (e->nunits > 0) {
+    if (priv == 0) rc = launch_match<0>(e, mp, smem, st);
+    else if (priv == 1) rc = launch_match<1>(e, mp, smem, st);
+    else rc = launch_match<2>(e, mp, smem, st);
+    if (rc != NGAP_OK) return rc;
+    e->launches++;
+  }
+  CUDA_TRY(cudaEventRecord(e->ev[2], st));
+  if (!p->report_off) {
+    int off_bits = bits_for(total);
+    int id_bits = 22 + bits_for((uint64_t)std::max(t->num_groups, 1));
+    rc = sort_unique(e, e->d_reports, e->d_counters + 0, cap, off_bits, id_bits, e->d_unique,
+                     e->d_counters + 1, st);
+    if (rc != NGAP_OK) return rc;
+  }
+  CUDA_TRY(cudaEventRecord(e->ev[3], st));
+  CUDA_TRY(cudaMemcpyAsync(e->h_counters, e->d_counters, 4 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(e->h_counters + 4, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  e->ran = true;
+  return NGAP_OK;
+}
+
+int ngap_engine_sync(ngap_engine* e) {
+  if (!e || !e->ran) {
+    set_error("ngap_engine_sync: no match in flight");
+    return NGAP_E_INVALID;
+  }
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaEventElapsedTime(&e->match_ms, e->ev[1], e->ev[2]));
+  CUDA_TRY(cudaEventElapsedTime(&e->sort_ms, e->ev[2], e->ev[3]));
+  int err = (int)(e->h_counters[4] & 0xffffffffull);
+  if (err & kErrTimeout) {
+    set_error("a bounded device wait gave up; results are incomplete");
+    return NGAP_E_TIMEOUT;
+  }
+  if (err & (kErrQueue | kErrCarry)) {
+    set_error("a worklist overflowed its capacity; results are incomplete");
+    return NGAP_E_OVERFLOW_QUEUE;
+  }
+  if (err & kErrResults) {
+    set_error("%llu reports exceed the result capacity of %llu; results are truncated",
+              (unsigned long long)e->h_counters[0], (unsigned long long)e->rep_cap);
+    return NGAP_E_OVERFLOW_RESULTS;
+  }
+  return NGAP_OK;
+}
+
+int ngap_results_count(const ngap_engine* e, uint64_t* raw, uint64_t* unique) {
+  if (!e) return NGAP_E_INVALID;
+  if (raw) *raw = e->h_counters[0];
+  if (unique) *unique = e->h_counters[1];
+  return NGAP_OK;
+}
+
+const uint64_t* ngap_results_device(const ngap_engine* e) { return e ? e->d_unique : nullptr; }
+
+int64_t ngap_results_copy(ngap_engine* e, uint64_t* host, uint64_t cap) {
+  if (!e || !host) return -1;
+  uint64_t n = std::min<uint64_t>(e->h_counters[1], cap);
+  if (n == 0) return 0;
+  if (cudaSetDevice(e->device) != cudaSuccess) return -1;
+  cudaError_t ce = cudaMemcpy(host, e->d_unique, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+  if (ce != cudaSuccess) {
+    set_error("cudaMemcpy: %s", cudaGetErrorString(ce));
+    return -1;
+  }
+  return (int64_t)n;
+}
+
+int ngap_last_times_ms(const ngap_engine* e, float* match_ms, float* sort_ms) {
+  if (!e) return NGAP_E_INVALID;
+  if (match_ms) *match_ms = e->match_ms;
+  if (sort_ms) *sort_ms = e->sort_ms;
+  return NGAP_OK;
+}
+
+int ngap_last_launches(const ngap_engine* e) { return e ? e->launches : 0; }
+
+int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injected) {
+  if (!e) return NGAP_E_INVALID;
+  if (expanded) *expanded = e->h_counters[2];
+  if (injected) *injected = e->h_counters[3];
+  return NGAP_OK;
+}
+
+int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                             uint64_t* n_out, void* stream) {
+  if (!e || (!d_in && n) || !d_out || !n_out) {
+    set_error("ngap_reports_sort_unique: null argument");
+    return NGAP_E_INVALID;
+  }
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  *n_out = 0;
+  if (n == 0) return NGAP_OK;
+  int rc = ensure_reports(e, n);
+  if (rc != NGAP_OK) return rc;
+  // input arrives in the reference encoding (id << 32 | offset): swap halves
+  // into sort keys in the engine's report buffer
+  CUDA_TRY(cudaMemcpyAsync(e->d_reports, d_in, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  unsigned long long hn = n;
+  CUDA_TRY(cudaMemcpyAsync(e->d_counters + 5, &hn, sizeof(hn), cudaMemcpyHostToDevice, st));
+  swap_halves<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 4096)), 256, 0, st>>>(e->d_reports, n);
+  CUDA_TRY(cudaGetLastError());
+  rc = sort_unique(e, e->d_reports, e->d_counters + 5, n, 32, 32, d_out, e->d_counters + 6, st);
+  if (rc != NGAP_OK) return rc;
+  unsigned long long un = 0;
+  CUDA_TRY(cudaMemcpyAsync(&un, e->d_counters + 6, sizeof(un), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  *n_out = un;
+  return NGAP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,344 @@
+"""Python mirror of the reference's `ngap` host interface over the C ABI.
+
+The reference drives matching through `class ngap` (code/src/ngap/ngap.h:27-177):
+set_ngap_option, preprocessing, set_nfa_group, add_symbol_stream,
+prepare_original_input_streams and one launch_*_groups() per algorithm. The
+same flow is offered here by :class:`Ngap`; :class:`Nfa`, :class:`Groups`,
+:class:`Tables` and :class:`Engine` wrap the C ABI objects one to one.
+"""
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import ALGORITHMS, NgapError, check, lib
+
+
+class Nfa:
+    """Parsed ANML (load_nfa_from_anml, code/src/commons/NFALoader.cpp:70)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def from_file(cls, path):
+        h = ctypes.c_void_p()
+        check(lib().ngap_nfa_load_anml(str(path).encode(), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_string(cls, xml):
+        data = xml.encode() if isinstance(xml, str) else bytes(xml)
+        h = ctypes.c_void_p()
+        check(lib().ngap_nfa_parse_anml(data, len(data), ctypes.byref(h)))
+        return cls(h.value)
+
+    @property
+    def num_states(self):
+        return lib().ngap_nfa_num_states(self._h)
+
+    @property
+    def num_edges(self):
+        return lib().ngap_nfa_num_edges(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
+            _lib._lib.ngap_nfa_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+@dataclass
+class GroupGraph:
+    """One group graph as Graph::ReadNFA + Csr::fromCoo lay it out."""
+    row_offsets: np.ndarray
+    col_indices: np.ndarray
+    symbol_sets: np.ndarray  # (V, 8) uint32
+    node_attrs: np.ndarray
+    always_active: np.ndarray
+    start_states: np.ndarray
+    cc_begin: np.ndarray
+    orig_node: np.ndarray
+
+    @property
+    def num_states(self):
+        return len(self.node_attrs)
+
+
+def _np(ptr, n, dtype):
+    if n == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+class Groups:
+    """Group graphs after CC split, degree limiting and grouping (ngap.cu:63-91)."""
+
+    def __init__(self, nfa, group_num=10, max_nfa_size=-1, quit_degree=True, remove_degree=False):
+        opts = _lib.GroupOpts(group_num, max_nfa_size, int(quit_degree), int(remove_degree))
+        h = ctypes.c_void_p()
+        check(lib().ngap_groups_build(nfa._h, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self._nfa = nfa
+
+    @property
+    def count(self):
+        return lib().ngap_groups_count(self._h)
+
+    def cc_stats(self):
+        t, f, b = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().ngap_groups_cc_stats(self._h, ctypes.byref(t), ctypes.byref(f), ctypes.byref(b)))
+        return t.value, f.value, b.value
+
+    def view(self, g):
+        v = _lib.GroupView()
+        check(lib().ngap_group_view_get(self._h, g, ctypes.byref(v)))
+        V, E = v.num_states, v.num_edges
+        return GroupGraph(
+            row_offsets=_np(v.row_offsets, V + 1, np.int32),
+            col_indices=_np(v.col_indices, E, np.int32),
+            symbol_sets=_np(v.symbol_sets, V * 8, np.uint32).reshape(V, 8),
+            node_attrs=_np(v.node_attrs, V, np.uint8),
+            always_active=_np(v.always_active, v.num_aas, np.int32),
+            start_states=_np(v.start_states, v.num_start, np.int32),
+            cc_begin=_np(v.cc_begin, v.num_ccs + 1, np.int32),
+            orig_node=_np(v.orig_node, V, np.int32),
+        )
+
+    def views(self):
+        return [self.view(g) for g in range(self.count)]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
+            _lib._lib.ngap_groups_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+class Tables:
+    """Device-resident matching tables (group_graph.h:6-109, ngap.cu:3086-3111)."""
+
+    def __init__(self, groups, device=0, precompute_depth=0, precompute_cutoff=-1,
+                 tile_states=0, max_table_entries=0):
+        opts = _lib.TableOpts(device, precompute_depth, precompute_cutoff, tile_states,
+                              max_table_entries)
+        h = ctypes.c_void_p()
+        check(lib().ngap_tables_build(groups._h, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self.groups = groups
+        self.num_groups = groups.count
+
+    @property
+    def device_bytes(self):
+        return lib().ngap_tables_device_bytes(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
+            _lib._lib.ngap_tables_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+class Engine:
+    """Device buffers, kernels and results (ngap_buffer.cu; ngap.cu launch_*)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(lib().ngap_engine_create(device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    def match_async(self, tables, data, num_seg, seg_len, algorithm="nonblockingallgroups",
+                    is_dup=False, unique=False, active_threshold=20, report_off=False,
+                    result_capacity=54619400, window=0, chunk=0, stream=None):
+        """Starts matching `data` (numpy uint8 array in host memory, or a CUDA
+        tensor / object exposing data_ptr()) of num_seg * seg_len bytes."""
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        p = _lib.MatchParams(algo, num_seg, seg_len, int(is_dup), int(unique), active_threshold,
+                             int(report_off), result_capacity, window, chunk)
+        if hasattr(data, "data_ptr"):
+            ptr, on_dev = data.data_ptr(), int(getattr(data, "is_cuda", True))
+        else:
+            arr = np.ascontiguousarray(data, dtype=np.uint8)
+            self._keep = arr
+            ptr, on_dev = arr.ctypes.data, 0
+        if num_seg * seg_len > 0 and ptr == 0:
+            raise NgapError(1, "empty input")
+        check(lib().ngap_match(self._h, tables._h, ctypes.c_void_p(ptr), on_dev, ctypes.byref(p),
+                               ctypes.c_void_p(stream or 0)))
+
+    def sync(self):
+        return check(lib().ngap_engine_sync(self._h))
+
+    def match(self, tables, data, num_seg, seg_len, **kw):
+        self.match_async(tables, data, num_seg, seg_len, **kw)
+        self.sync()
+        return self.results()
+
+    def counts(self):
+        raw, uniq = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().ngap_results_count(self._h, ctypes.byref(raw), ctypes.byref(uniq)))
+        return raw.value, uniq.value
+
+    def results(self):
+        """Sorted unique reports, reference encoding ((sid|g<<22)<<32 | offset)."""
+        _, n = self.counts()
+        out = np.zeros(n, dtype=np.uint64)
+        if n:
+            got = lib().ngap_results_copy(self._h, out.ctypes.data, n)
+            if got != n:
+                raise NgapError(5, _lib.last_error())
+        return out
+
+    def results_device_ptr(self):
+        return lib().ngap_results_device(self._h)
+
+    def times_ms(self):
+        a, b = ctypes.c_float(), ctypes.c_float()
+        check(lib().ngap_last_times_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def launches(self):
+        return lib().ngap_last_launches(self._h)
+
+    def work(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().ngap_engine_work(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def sort_unique_device(self, d_in_ptr, n, d_out_ptr, stream=None):
+        """Device radix sort + unique of n reference-encoded reports."""
+        nout = ctypes.c_uint64()
+        check(lib().ngap_reports_sort_unique(self._h, ctypes.c_void_p(d_in_ptr), n,
+                                             ctypes.c_void_p(d_out_ptr), ctypes.byref(nout),
+                                             ctypes.c_void_p(stream or 0)))
+        return nout.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
+            _lib._lib.ngap_engine_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+def cpu_validate(groups, data, num_seg, seg_len, is_dup=False):
+    """The library's CPU checker (the CLI's --validation): sorted unique reports."""
+    arr = np.ascontiguousarray(data, dtype=np.uint8)
+    cap = 1 << 16
+    while True:
+        out = np.zeros(cap, dtype=np.uint64)
+        ms = ctypes.c_double()
+        n = lib().ngap_cpu_validate_reference(groups._h, arr.ctypes.data, num_seg, seg_len,
+                                              int(is_dup), out.ctypes.data, cap, ctypes.byref(ms))
+        if n >= 0:
+            return out[:n]
+        cap *= 4
+
+
+@dataclass
+class NgapOption:
+    """Fields and defaults of ngap_option + common_gpunfa_options
+    (code/src/ngap/ngap_option.h:52-68, code/include/commons/common_func.h:50-58)."""
+    algorithm: str = "nonblockingallgroups"
+    group_num: int = 10
+    max_nfa_size: int = -1
+    quit_degree: bool = True
+    remove_degree: bool = False
+    duplicate_input_stream: int = 1
+    input_start_pos: int = 0
+    input_len: int = -1
+    split_chunk_size: int = -1
+    output_capacity: int = 54619400
+    report_off: bool = False
+    unique: bool = False
+    active_threshold: int = 20
+    precompute_depth: int = 0
+    precompute_cutoff: int = -1
+    data_buffer_fetch_size: int = 128
+    add_aas_start: int = 0
+    add_aas_interval: int = 1
+    validation: bool = True
+    quick_validation: int = -1
+    device: int = 0
+    window: int = 0
+    chunk: int = 0
+    tile_states: int = 0
+
+
+class Ngap:
+    """Reference-shaped driver: the main.cu flow on one GPU."""
+
+    def __init__(self, nfa, opt=None):
+        self.nfa = nfa
+        self.opt = opt or NgapOption()
+        self.groups = None
+        self.tables = None
+        self.streams = []
+        self.engine = None
+
+    def set_ngap_option(self, opt):
+        self.opt = opt
+
+    def preprocessing(self):
+        o = self.opt
+        self.groups = Groups(self.nfa, o.group_num, o.max_nfa_size, o.quit_degree, o.remove_degree)
+        self.opt.group_num = self.groups.count
+        return self.groups
+
+    def add_symbol_stream(self, seg):
+        self.streams.append(np.ascontiguousarray(seg, dtype=np.uint8))
+
+    def prepare_segments(self, data):
+        """main.cu:81-102: duplicate, then cut into equal segments."""
+        o = self.opt
+        ss = np.tile(np.ascontiguousarray(data, dtype=np.uint8), o.duplicate_input_stream)
+        chunk = o.split_chunk_size if o.split_chunk_size > 0 else len(ss)
+        num_seg = len(ss) // chunk
+        self.streams = [ss[i * chunk:(i + 1) * chunk] for i in range(num_seg)]
+        return num_seg, chunk
+
+    def is_dup(self):
+        o = self.opt
+        return o.duplicate_input_stream > 1 and (o.split_chunk_size in (-1, o.input_len))
+
+    def launch(self, algorithm=None):
+        o = self.opt
+        if self.groups is None:
+            self.preprocessing()
+        if self.tables is None:
+            self.tables = Tables(self.groups, o.device, o.precompute_depth, o.precompute_cutoff,
+                                 o.tile_states)
+        if self.engine is None:
+            self.engine = Engine(o.device)
+        data = np.concatenate(self.streams) if self.streams else np.zeros(0, np.uint8)
+        seg_len = len(self.streams[0]) if self.streams else 0
+        return self.engine.match(self.tables, data, len(self.streams), seg_len,
+                                 algorithm=algorithm or o.algorithm, is_dup=self.is_dup(),
+                                 unique=o.unique, active_threshold=o.active_threshold,
+                                 report_off=o.report_off, result_capacity=o.output_capacity,
+                                 window=o.window, chunk=o.chunk)
+
+    # one entry point per reference launcher (main.cu:114-127)
+    def launch_blocking_groups(self):
+        return self.launch("blockinggroups")
+
+    def launch_non_blocking_nap_groups(self):
+        return self.launch("NAPgroups")
+
+    def launch_non_blocking_groups(self):
+        return self.launch("nonblockinggroups")
+
+    def launch_non_blocking_r1_groups(self):
+        return self.launch("nonblockingr1groups")
+
+    def launch_non_blocking_r2_groups(self):
+        return self.launch("nonblockingr2groups")
+
+    def launch_non_blocking_prec_groups(self):
+        return self.launch("nonblockingpcgroups")
+
+    def launch_non_blocking_all_groups(self):
+        return self.launch("nonblockingallgroups")
+
+
+def decode_reports(reports):
+    """Splits reference-encoded reports into (ids, offsets)."""
+    r = np.asarray(reports, dtype=np.uint64)
+    return (r >> np.uint64(32)).astype(np.uint32), (r & np.uint64(0xFFFFFFFF)).astype(np.uint32)

@@ -1,0 +1,161 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+Every case compares the sorted, deduplicated (offset, id) reports of the
+engine with the oracle's restatement of the reference CPU matcher
+(code/src/ngap/ngap.cu:2171-2344) on the same seeded input: bit-exact.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ngap_b200 as nb
+from ngap_b200 import workloads as W
+from oracle import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+ALGOS = list(nb.ALGORITHMS)
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(engine, anml, data, num_seg, seg_len, group_num=1, depth=0, is_dup=False, **kw):
+    nfa = nb.Nfa.from_string(anml)
+    groups = nb.Groups(nfa, group_num=group_num)
+    tables = nb.Tables(groups, precompute_depth=depth, tile_states=kw.pop("tile_states", 0))
+    got = engine.match(tables, data[:num_seg * seg_len], num_seg, seg_len, is_dup=is_dup, **kw)
+    want, _ = oracle.match(groups.views(), data[:num_seg * seg_len], num_seg, seg_len,
+                           is_dup=is_dup)
+    return got, want
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_apple_known_answer(engine, algo):
+    """README.md:156-186: state 4 reports at offsets 5, 47, 64 and 75."""
+    anml = open(os.path.join(GOLD, "apple.anml")).read()
+    data = np.fromfile(os.path.join(GOLD, "apple_input.txt"), dtype=np.uint8)
+    got, want = run_both(engine, anml, data, 1, len(data), depth=3, algorithm=algo)
+    assert [hex(x) for x in got] == ["0x400000005", "0x40000002f", "0x400000040", "0x40000004b"]
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("num_seg,group_num,depth", [(1, 1, 0), (4, 3, 2), (8, 10, 3)])
+def test_literal_set(engine, algo, num_seg, group_num, depth):
+    anml, data = W.literal_set(seed=5, input_len=1 << 18, plant_every=1 << 12)
+    seg = len(data) // num_seg
+    got, want = run_both(engine, anml, data, num_seg, seg, group_num=group_num, depth=depth,
+                         algorithm=algo)
+    assert len(want) > 10
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("algo", ["blockinggroups", "nonblockinggroups", "nonblockingpcgroups",
+                                  "nonblockingallgroups", "nonblockingr2groups"])
+def test_hamming(engine, algo):
+    anml, data = W.hamming_set(seed=7, n_patterns=60, input_len=1 << 18, plant_every=1 << 11)
+    got, want = run_both(engine, anml, data, 4, len(data) // 4, group_num=4, depth=3,
+                         algorithm=algo)
+    assert len(want) > 50
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("algo", ["NAPgroups", "nonblockinggroups", "nonblockingallgroups"])
+def test_levenshtein_degree_limited(engine, algo):
+    anml, data = W.levenshtein_set(seed=8, n_patterns=40, input_len=1 << 17, plant_every=1 << 11)
+    got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=5, depth=2,
+                         algorithm=algo)
+    assert len(want) > 20
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("algo", ["blockinggroups", "nonblockinggroups", "nonblockingallgroups"])
+@pytest.mark.parametrize("window", [0, 64])
+def test_dotstar_unbounded(engine, algo, window):
+    """`.*` states with self-loops make tiles unbounded (one unit per segment,
+    carried across windows)."""
+    anml, data = W.dotstar_set(seed=9, n_patterns=150, input_len=1 << 17, plant_every=1 << 11)
+    got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=3, depth=3,
+                         algorithm=algo, window=window)
+    assert len(want) > 20
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("chunk,window,tile_states", [(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
+def test_chunking_and_tiling(engine, chunk, window, tile_states):
+    """Small chunks, windows and tiles exercise warm-up, carry and tile splits."""
+    anml, data = W.hamming_set(seed=12, n_patterns=30, input_len=1 << 16, plant_every=1 << 10)
+    got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=3, depth=2,
+                         algorithm="nonblockingallgroups", chunk=chunk, window=window,
+                         tile_states=tile_states)
+    assert np.array_equal(got, want)
+
+
+def test_start_of_data_and_dup(engine):
+    """Start-of-data states: segment 0 only, or every segment when duplicated."""
+    anml = W.AnmlWriter()
+    anml.ste("a", [ord("x")], ["b"], start="start-of-data")
+    anml.ste("b", [ord("y")], ["c"])
+    anml.ste("c", [ord("z")], [], report=True)
+    anml.ste("d", [ord("y")], ["e"], start="all-input")
+    anml.ste("e", [ord("z")], [], report=True)
+    data = np.frombuffer(b"xyzxyz" * 4, dtype=np.uint8).copy()
+    for is_dup in (False, True):
+        for algo in ALGOS:
+            got, want = run_both(engine, anml.text(), data, 4, 6, group_num=2, is_dup=is_dup,
+                                 depth=2, algorithm=algo)
+            assert np.array_equal(got, want), (algo, is_dup)
+
+
+@pytest.mark.parametrize("seg_len", [1, 2, 3, 17])
+def test_ragged_tiny_segments(engine, seg_len):
+    anml, data = W.literal_set(seed=13, n_patterns=20, len_lo=1, len_hi=3, input_len=1 << 12,
+                               plant_every=64)
+    n = len(data) // seg_len
+    got, want = run_both(engine, anml, data, n, seg_len, group_num=2, depth=3,
+                         algorithm="nonblockingallgroups")
+    assert np.array_equal(got, want)
+
+
+def test_unique_flag(engine):
+    anml, data = W.levenshtein_set(seed=14, n_patterns=20, input_len=1 << 15, plant_every=1 << 10)
+    got, want = run_both(engine, anml, data, 1, len(data), group_num=2, depth=1,
+                         algorithm="nonblockinggroups", unique=True)
+    assert np.array_equal(got, want)
+
+
+def test_report_off_and_capacity(engine):
+    anml, data = W.literal_set(seed=15, input_len=1 << 16, plant_every=1 << 9)
+    nfa = nb.Nfa.from_string(anml)
+    groups = nb.Groups(nfa, group_num=1)
+    tables = nb.Tables(groups, precompute_depth=1)
+    want, _ = oracle.match(groups.views(), data, 1, len(data))
+    engine.match(tables, data, 1, len(data), report_off=True)
+    raw, uniq = engine.counts()
+    assert raw >= len(want) and uniq == 0
+    with pytest.raises(nb.NgapError) as ei:
+        engine.match(tables, data, 1, len(data), result_capacity=3)
+    assert ei.value.status == 7  # NGAP_E_OVERFLOW_RESULTS
+
+
+def test_device_input_and_sort_api(engine):
+    import torch
+    anml, data = W.hamming_set(seed=16, n_patterns=20, input_len=1 << 16, plant_every=1 << 10)
+    nfa = nb.Nfa.from_string(anml)
+    groups = nb.Groups(nfa, group_num=2)
+    tables = nb.Tables(groups, precompute_depth=3)
+    d = torch.from_numpy(data).cuda()
+    got = engine.match(tables, d, 4, len(data) // 4)
+    want, _ = oracle.match(groups.views(), data, 4, len(data) // 4)
+    assert np.array_equal(got, want)
+    # the standalone radix sort + unique on a shuffled, duplicated copy
+    rng = np.random.default_rng(0)
+    shuffled = np.concatenate([want, want[: len(want) // 2]])
+    rng.shuffle(shuffled)
+    din = torch.from_numpy(shuffled.view(np.int64)).cuda()
+    dout = torch.empty_like(din)
+    n = engine.sort_unique_device(din.data_ptr(), len(shuffled), dout.data_ptr())
+    torch.cuda.synchronize()
+    assert n == len(want)
+    assert np.array_equal(dout[:n].cpu().numpy().view(np.uint64), want)
