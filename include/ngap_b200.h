@@ -163,6 +163,23 @@ int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injecte
 int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
                              uint64_t* n_out, void* stream);
 
+/* Same sort + unique as ngap_reports_sort_unique, but allocating nothing: it
+ * has no counterpart in the reference. It is for callers that cannot call
+ * cudaMalloc — a process whose device memory is owned by another allocator
+ * (for example a framework's caching allocator that has reserved the GPU), or
+ * a latency-critical loop where cudaMalloc's implicit synchronisation is not
+ * acceptable. The caller passes device input (n reference-encoded reports)
+ * and device output (room for n); n must not exceed 262,144 (larger n returns
+ * NGAP_E_INVALID). Scratch (about 2 MiB) is a static device array that every
+ * GPU loading this library keeps until exit. The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device
+ * current, so make the first call before any stream capture. All calls share
+ * the scratch and it keeps the last call's contents; calls that overlap on
+ * the GPU race on it. Uses the calling thread's current device; waits for
+ * `stream` before returning the unique count in *n_out. */
+int ngap_reports_sort_unique_noalloc(const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                                     uint64_t* n_out, void* stream);
+
 /* ---- CPU checker used by the CLI's --validation (ngap.cu:2171-2344) ---- */
 
 /* Runs the reference's CPU frontier simulation over the group graphs and

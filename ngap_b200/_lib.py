@@ -100,6 +100,10 @@ SIGNATURES = {
     "ngap_reports_sort_unique": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                                 ctypes.c_void_p]),
+    "ngap_reports_sort_unique_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                                        ctypes.c_void_p,
+                                                        ctypes.POINTER(ctypes.c_uint64),
+                                                        ctypes.c_void_p]),
     "ngap_cpu_validate_reference": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                                      ctypes.c_void_p, ctypes.c_int64,

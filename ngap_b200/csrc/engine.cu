@@ -632,3 +632,127 @@ int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, u
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Report sort + unique without any device allocation.
+//
+// Some callers cannot call cudaMalloc: a serving process whose device memory
+// is owned by another allocator (a framework's caching allocator that has
+// reserved the GPU), or a latency-critical loop where cudaMalloc's implicit
+// device synchronisation is not acceptable. For them the scratch of the
+// report sort lives in the file-scope array below, reserved on every GPU that
+// loads this library until the process exits. It holds one ping-pong key
+// buffer of kNoAllocMaxReports entries plus the digit histograms and
+// counters (about 2 MiB). All calls share it and it keeps the last call's
+// contents: calls whose work overlaps on the GPU (other streams, other host
+// threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr uint64_t kNoAllocMaxReports = 1ull << 18;  // 262,144 reports
+constexpr uint64_t kNoAllocTiles = (kNoAllocMaxReports + kSortTile - 1) / kSortTile;
+constexpr size_t kNoAllocKeyBytes = kNoAllocMaxReports * sizeof(uint64_t);
+constexpr size_t kNoAllocHistBytes = 16 * kNoAllocTiles * sizeof(uint32_t);
+constexpr size_t kNoAllocBytes = kNoAllocKeyBytes + kNoAllocHistBytes + 4 * sizeof(unsigned long long);
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+uint8_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device. In host code
+// g_noalloc_scratch names a host-side stand-in, not device memory, so the
+// address is looked up once per device with that device current.
+int noalloc_scratch(int dev, uint8_t** out) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_error("device %d is beyond the %d devices the allocation-free path supports", dev,
+              kNoAllocMaxDevices);
+    return NGAP_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (ce != cudaSuccess) {
+      set_error("cudaGetSymbolAddress of the sort scratch failed: %s", cudaGetErrorString(ce));
+      return NGAP_E_CUDA;
+    }
+    g_noalloc_addr[dev] = static_cast<uint8_t*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return NGAP_OK;
+}
+
+// Copies reference-encoded reports into sort keys (offset << 32 | id) and
+// resets the counters: [0] = n, [1] = unique count.
+__global__ void noalloc_prepare(const uint64_t* __restrict__ in, uint64_t n,
+                                uint64_t* __restrict__ keys, unsigned long long* counters) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = n;
+    counters[1] = 0;
+    counters[2] = 0;
+    counters[3] = 0;
+  }
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t x = in[i];
+    keys[i] = (x << 32) | (x >> 32);
+  }
+}
+
+}  // namespace
+
+extern "C" int ngap_reports_sort_unique_noalloc(const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                                                uint64_t* n_out, void* stream) {
+  if ((!d_in && n) || !d_out || !n_out) {
+    set_error("ngap_reports_sort_unique_noalloc: null argument");
+    return NGAP_E_INVALID;
+  }
+  if (n > kNoAllocMaxReports) {
+    set_error("ngap_reports_sort_unique_noalloc: %llu reports exceed the allocation-free "
+              "maximum of %llu", (unsigned long long)n, (unsigned long long)kNoAllocMaxReports);
+    return NGAP_E_INVALID;
+  }
+  *n_out = 0;
+  if (n == 0) return NGAP_OK;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  uint8_t* base = nullptr;
+  int rc = noalloc_scratch(dev, &base);
+  if (rc != NGAP_OK) return rc;
+  uint64_t* keys = reinterpret_cast<uint64_t*>(base);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + kNoAllocKeyBytes);
+  unsigned long long* counters =
+      reinterpret_cast<unsigned long long*>(base + kNoAllocKeyBytes + kNoAllocHistBytes);
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(tiles, (uint32_t)sms * 8));
+  // 8 digit passes over the offset half and 8 over the id half; an even count
+  // leaves the sorted keys back in the scratch buffer, d_out being the other
+  // half of the ping-pong
+  const int npass = 16;
+  uint64_t* src = (npass % 2 == 0) ? keys : d_out;
+  uint64_t* dst = (npass % 2 == 0) ? d_out : keys;
+  noalloc_prepare<<<grid, 256, 0, st>>>(d_in, n, src, counters);
+  for (int k = 0; k < npass; k++) {
+    const int sh = k < 8 ? 4 * k : 32 + 4 * (k - 8);
+    radix_hist<<<grid, kSortThreads, 0, st>>>(src, counters, n, sh, hist);
+    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(hist, counters, n, 16, nullptr);
+    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, counters, n, sh, hist);
+    std::swap(src, dst);
+  }
+  unique_count<<<grid, kSortThreads, 0, st>>>(src, counters, n, hist);
+  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(hist, counters, n, 1, counters + 1);
+  unique_write<<<grid, kSortThreads, 0, st>>>(src, counters, n, hist, d_out);
+  CUDA_TRY(cudaGetLastError());
+  unsigned long long un = 0;
+  CUDA_TRY(cudaMemcpyAsync(&un, counters + 1, sizeof(un), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  *n_out = un;
+  return NGAP_OK;
+}
