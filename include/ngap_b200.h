@@ -130,6 +130,9 @@ typedef struct ngap_match_params {
   uint64_t result_capacity;  /* --result-capacity */
   int window;                /* positions per worklist window; 0 = automatic */
   int chunk;                 /* positions per chunk of a bounded tile; 0 = automatic */
+  int64_t first_segment;     /* global index of the first segment when a stream is
+                                split across GPUs (start-of-data states belong to
+                                global segment 0); 0 otherwise */
 } ngap_match_params;
 
 /* Replaces ngap::launch_*_groups (code/src/ngap/ngap.cu:115-2078) up to the

@@ -59,7 +59,7 @@ class MatchParams(ctypes.Structure):
                 ("seg_len", ctypes.c_int64), ("is_dup", ctypes.c_int), ("unique", ctypes.c_int),
                 ("active_threshold", ctypes.c_int), ("report_off", ctypes.c_int),
                 ("result_capacity", ctypes.c_uint64), ("window", ctypes.c_int),
-                ("chunk", ctypes.c_int)]
+                ("chunk", ctypes.c_int), ("first_segment", ctypes.c_int64)]
 
 
 # name -> (restype, argtypes); exactly the functions include/ngap_b200.h declares

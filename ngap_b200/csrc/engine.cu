@@ -68,9 +68,10 @@ struct ngap_tables {
 struct UnitPlanKey {
   int64_t num_seg, seg_len;
   int is_dup, window, chunk;
+  int64_t first_seg;
   bool operator<(const UnitPlanKey& o) const {
-    return std::tie(num_seg, seg_len, is_dup, window, chunk) <
-           std::tie(o.num_seg, o.seg_len, o.is_dup, o.window, o.chunk);
+    return std::tie(num_seg, seg_len, is_dup, window, chunk, first_seg) <
+           std::tie(o.num_seg, o.seg_len, o.is_dup, o.window, o.chunk, o.first_seg);
   }
 };
 
@@ -83,7 +84,7 @@ struct ngap_engine {
   size_t input_cap = 0;
   // units (cached plan for one tables object)
   const ngap_tables* plan_tables = nullptr;
-  UnitPlanKey plan_key{-1, -1, -1, -1, -1};
+  UnitPlanKey plan_key{-1, -1, -1, -1, -1, -1};
   UnitDev* d_units = nullptr;
   size_t units_cap = 0;
   int32_t nunits = 0;
@@ -295,7 +296,7 @@ void plan_units(const ngap_tables* t, const UnitPlanKey& k, std::vector<UnitDev>
     const TileHost& th = t->tiles[ti];
     for (int64_t s = 0; s < k.num_seg; s++) {
       const int64_t slo = s * k.seg_len, shi = slo + k.seg_len;
-      const bool starts = (s == 0 || k.is_dup) && !th.start.empty();
+      const bool starts = (k.first_seg + s == 0 || k.is_dup) && !th.start.empty();
       if (th.max_path < 0) {
         UnitDev u;
         u.tile = ti;
@@ -453,7 +454,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   int rc = ensure_reports(e, cap);
   if (rc != NGAP_OK) return rc;
   // units
-  UnitPlanKey key{p->num_seg, p->seg_len, p->is_dup ? 1 : 0, window, p->chunk};
+  UnitPlanKey key{p->num_seg, p->seg_len, p->is_dup ? 1 : 0, window, p->chunk, p->first_segment};
   if (e->plan_tables != t || key < e->plan_key || e->plan_key < key) {
     std::vector<UnitDev> units;
     plan_units(t, key, units);

@@ -148,12 +148,14 @@ class Engine:
 
     def match_async(self, tables, data, num_seg, seg_len, algorithm="nonblockingallgroups",
                     is_dup=False, unique=False, active_threshold=20, report_off=False,
-                    result_capacity=54619400, window=0, chunk=0, stream=None):
+                    result_capacity=54619400, window=0, chunk=0, first_segment=0, stream=None):
         """Starts matching `data` (numpy uint8 array in host memory, or a CUDA
-        tensor / object exposing data_ptr()) of num_seg * seg_len bytes."""
+        tensor / object exposing data_ptr()) of num_seg * seg_len bytes.
+        first_segment: global index of data's first segment when a stream is
+        split across GPUs (start-of-data states belong to global segment 0)."""
         algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
         p = _lib.MatchParams(algo, num_seg, seg_len, int(is_dup), int(unique), active_threshold,
-                             int(report_off), result_capacity, window, chunk)
+                             int(report_off), result_capacity, window, chunk, first_segment)
         if hasattr(data, "data_ptr"):
             ptr, on_dev = data.data_ptr(), int(getattr(data, "is_cuda", True))
         else:

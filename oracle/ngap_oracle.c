@@ -62,14 +62,14 @@ static inline int accepts(const oracle_group* g, int32_t v, uint8_t s) {
 static inline uint64_t to_key(uint32_t id, uint32_t off) { return ((uint64_t)off << 32) | id; }
 
 static void run_unit(const oracle_group* g, int gi, const uint8_t* input, int64_t seg,
-                     int64_t seg_len, int is_dup, int mode, int unique, vec64* rep,
-                     oracle_stats* st) {
+                     int64_t seg_len, int is_dup, int64_t first_seg, int mode, int unique,
+                     vec64* rep, oracle_stats* st) {
   const int64_t lo = seg * seg_len, hi = lo + seg_len;
   const uint32_t gbits = (uint32_t)gi << 22;
   vec32 cur = {0}, nxt = {0};
   uint8_t* mark = NULL;
   if (mode == 1) mark = (uint8_t*)calloc((size_t)g->V + 1, 1);
-  if (seg == 0 || is_dup)
+  if (first_seg + seg == 0 || is_dup)
     for (int i = 0; i < g->nstart; i++) vpush32(&cur, g->starts[i]);
   for (int i = 0; i < g->naas; i++) vpush32(&cur, g->aas[i]);
   if (mode == 1) { /* deduplicate the initial frontier */
@@ -138,8 +138,8 @@ static int64_t g_last_needed = 0;
 int64_t oracle_last_needed(void) { return g_last_needed; }
 
 int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* input,
-                     int64_t num_seg, int64_t seg_len, int is_dup, int mode, int unique,
-                     int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats) {
+                     int64_t num_seg, int64_t seg_len, int is_dup, int64_t first_seg, int mode,
+                     int unique, int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats) {
   const int64_t units = (int64_t)ngroups * num_seg;
   vec64* reps = (vec64*)calloc((size_t)(units > 0 ? units : 1), sizeof(vec64));
   oracle_stats* sts = (oracle_stats*)calloc((size_t)(units > 0 ? units : 1), sizeof(oracle_stats));
@@ -148,7 +148,8 @@ int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* inp
   for (int64_t u = 0; u < units; u++) {
     int gi = (int)(u / num_seg);
     int64_t seg = u % num_seg;
-    run_unit(&groups[gi], gi, input, seg, seg_len, is_dup, mode, unique, &reps[u], &sts[u]);
+    run_unit(&groups[gi], gi, input, seg, seg_len, is_dup, first_seg, mode, unique, &reps[u],
+             &sts[u]);
   }
   int64_t total = 0;
   oracle_stats acc = {0, 0, 0, 0};

@@ -42,10 +42,12 @@ typedef struct oracle_stats {
  * Reports are written as the reference packs them, ((sid | g << 22) << 32) |
  * offset, sorted by (offset, id) and deduplicated. Returns the number of
  * unique reports, or -1 when more than `cap` would be written (stats and the
- * return of oracle_last_needed() still give the count). */
+ * return of oracle_last_needed() still give the count). first_seg is the
+ * global index of the first segment (start-of-data states belong to global
+ * segment 0 unless is_dup). */
 int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* input,
-                     int64_t num_seg, int64_t seg_len, int is_dup, int mode, int unique,
-                     int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats);
+                     int64_t num_seg, int64_t seg_len, int is_dup, int64_t first_seg, int mode,
+                     int unique, int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats);
 
 int64_t oracle_last_needed(void);
 

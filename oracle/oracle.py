@@ -43,9 +43,9 @@ def lib():
         L = ctypes.CDLL(LIB)
         L.oracle_match.restype = ctypes.c_int64
         L.oracle_match.argtypes = [ctypes.POINTER(OracleGroup), ctypes.c_int, ctypes.c_void_p,
-                                   ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
-                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
-                                   ctypes.POINTER(OracleStats)]
+                                   ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_int64, ctypes.POINTER(OracleStats)]
         L.oracle_last_needed.restype = ctypes.c_int64
         _L = L
     return _L
@@ -57,7 +57,8 @@ def _field(g, name):
     return getattr(g, name)
 
 
-def match(groups, data, num_seg, seg_len, is_dup=False, mode=1, unique=False, nthreads=0):
+def match(groups, data, num_seg, seg_len, is_dup=False, mode=1, unique=False, nthreads=0,
+          first_segment=0):
     """Returns (sorted unique reports as uint64 in the reference encoding, stats dict).
     `groups` items expose row_offsets, col_indices, symbol_sets, node_attrs,
     always_active, start_states (dicts or objects)."""
@@ -79,7 +80,7 @@ def match(groups, data, num_seg, seg_len, is_dup=False, mode=1, unique=False, nt
     while True:
         out = np.zeros(cap, dtype=np.uint64)
         n = lib().oracle_match(arr, len(groups), d.ctypes.data, num_seg, seg_len, int(is_dup),
-                               mode, int(unique), nthreads, out.ctypes.data, cap,
+                               first_segment, mode, int(unique), nthreads, out.ctypes.data, cap,
                                ctypes.byref(stats))
         if n >= 0:
             break

@@ -1,0 +1,70 @@
+"""The C-ABI library (CPU): loads, exports every declared symbol, and its
+host-only entry points work without a GPU. Also the CLI's argument handling."""
+import os
+import re
+import subprocess
+
+import pytest
+
+import ngap_b200 as nb
+from ngap_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ngap_b200.h")
+CLI = os.path.join(ROOT, "ngap_b200", "bin", "ngap")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w\s\*]*?\b(ngap_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_api():
+    names = declared_functions()
+    assert "ngap_match" in names and "ngap_reports_sort_unique_noalloc" in names
+    assert len(names) >= 25
+
+
+def test_library_exports_every_declared_symbol(built):
+    L = nb.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert missing == []
+
+
+def test_binding_covers_header(built):
+    assert sorted(_lib.SIGNATURES) == declared_functions()
+
+
+def test_host_entry_points_without_gpu(built):
+    nfa = nb.Nfa.from_string(open(os.path.join(ROOT, "tests", "golden", "apple.anml")).read())
+    assert (nfa.num_states, nfa.num_edges) == (5, 4)
+    g = nb.Groups(nfa, group_num=3)
+    assert g.count == 1 and g.cc_stats() == (1, 0, 0)
+    assert nb.lib().ngap_version().startswith(b"ngap_b200")
+
+
+def test_null_arguments_are_errors(built):
+    L = nb.lib()
+    assert L.ngap_nfa_load_anml(None, None) == 1
+    assert L.ngap_groups_build(None, None, None) == 1
+    assert L.ngap_match(None, None, None, 0, None, None) == 1
+    assert "null" in _lib.last_error()
+
+
+def test_cli_bad_args():
+    r = subprocess.run([CLI, "--bogus", "1"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Error in command line" in r.stderr
+    r = subprocess.run([CLI, "-a", "x.anml"], capture_output=True, text=True)
+    assert r.returncode == 1
+
+
+def test_cli_unknown_algorithm(tmp_path):
+    inp = tmp_path / "in.txt"
+    inp.write_bytes(b"apple" * 10)
+    r = subprocess.run([CLI, "-a", os.path.join(ROOT, "tests", "golden", "apple.anml"), "-i",
+                        str(inp), "--algorithm=nosuch", "--group-num=1"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0
+    assert "not supported algoritm nosuch" in r.stdout and "FINISHED!" in r.stdout
