@@ -12,15 +12,19 @@ constexpr int kMaxDepth = 3;         // prefix-memoization depth limit (referenc
 constexpr int kEntryPosBits = 13;    // worklist entry = local_state << 13 | window offset
 constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
 constexpr int kMaxTileStates = 1 << (32 - kEntryPosBits);
+constexpr int kDenseKeyBits = 16;    // prefix tables with keys of <= 16 bits are dense
 
 // One prefix-memoization table of depth d for a tile (precompute_table.h:8-101).
-// Key = d input bytes in base 256. dense: offsets indexed by key; otherwise
-// keys[] holds the sorted non-empty keys and offsets are indexed by rank.
+// The key is the class ids of the next d input bytes, kb bits each
+// (kb = TileDev::kb). dense: offsets indexed by the key; otherwise keys[]
+// holds the sorted non-empty keys and offsets are indexed by rank.
 struct PrefixTableDev {
   int32_t dense = 0;
   int32_t nkeys = 0;
   int32_t nrkeys = 0;
   int32_t cutoff = 0;
+  int32_t has_reports = 0;          // any report list non-empty
+  int32_t pad = 0;
   const uint32_t* keys = nullptr;   // state-list keys (compressed)
   const uint32_t* voff = nullptr;   // state-list offsets
   const uint32_t* vlist = nullptr;  // local states reached after d bytes
@@ -30,16 +34,26 @@ struct PrefixTableDev {
 };
 
 // A tile: a set of whole CCs of one group, matched by one warp per unit.
+// Its hot tables form one contiguous image, staged into shared memory by the
+// CTA that works on the tile:
+//   [succ: nstates x uint4][cmask: nstates x cw x u32][rep: ceil(nstates/32) x u32][cls: 256 B]
+// succ: up to 4 tile-local successors, bit 31 = successor is a report state,
+// kNoSucc = none. cmask: bit c of word c/32 = the state accepts byte class c.
+// cls: byte -> class (identity when cw == 8).
 struct TileDev {
   int32_t group = 0;
   int32_t nstates = 0;
   int32_t naas = 0;
   int32_t nstart = 0;
-  int32_t depth = 0;       // prefix depth used by this tile (0 = scan the AAS list)
-  int32_t max_path = -1;   // longest path in states if acyclic, else -1
-  const uint4* succ = nullptr;      // [nstates] local successors (edges into AAS removed)
-  const uint32_t* bits = nullptr;   // [nstates * 8] symbol classes
-  const uint32_t* rep = nullptr;    // [ceil(nstates / 32)] report bitmap
+  int32_t depth = 0;        // prefix depth built for this tile (>= 1)
+  int32_t max_path = -1;    // longest path in states if acyclic, else -1
+  int32_t ncls = 0;         // byte classes
+  int32_t cw = 8;           // class words per state: 1, 2 or 8
+  int32_t kb = 8;           // key bits per class symbol: 5, 6 or 8
+  int32_t image_bytes = 0;  // multiple of 16
+  int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
+  int32_t inj_batch = 32;   // positions injected per worklist refill
+  const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
   const uint32_t* sid = nullptr;    // [nstates] local -> group-local sid
   const uint32_t* aas = nullptr;    // [naas] local ids
   const uint32_t* start = nullptr;  // [nstart] local ids
@@ -52,6 +66,13 @@ struct UnitDev {
   int32_t tile;
   uint32_t flags;  // bit0: inject start-of-data states at lo
   int64_t lo, hi, emit_lo;
+};
+
+// A CTA-level task: consecutive units [ubegin, uend) of one tile.
+struct TaskDev {
+  int32_t tile;
+  int32_t ubegin, uend;
+  int32_t pad;
 };
 
 }  // namespace ngap

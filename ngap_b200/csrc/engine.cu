@@ -46,6 +46,7 @@ struct ngap_tables {
   std::vector<void*> allocs;
   int64_t bytes = 0;
   int32_t max_states = 0;
+  int32_t image_region = 0;  // shared-memory bytes reserved for tile images
 
   ~ngap_tables() {
     for (void* p : allocs) cudaFree(p);
@@ -88,6 +89,9 @@ struct ngap_engine {
   UnitDev* d_units = nullptr;
   size_t units_cap = 0;
   int32_t nunits = 0;
+  TaskDev* d_tasks = nullptr;
+  size_t tasks_cap = 0;
+  int32_t ntasks = 0;
   // reports
   uint64_t rep_cap = 0;
   uint64_t* d_reports = nullptr;
@@ -118,6 +122,7 @@ struct ngap_engine {
   ~ngap_engine() {
     cudaFree(d_input);
     cudaFree(d_units);
+    cudaFree(d_tasks);
     cudaFree(d_reports);
     cudaFree(d_tmp);
     cudaFree(d_unique);
@@ -174,11 +179,15 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.nstart = (int32_t)th.start.size();
     d.depth = th.depth;
     d.max_path = th.max_path;
-    const uint32_t* succ = nullptr;
-    if ((rc = t->upload(th.succ, &succ)) != NGAP_OK) return rc;
-    d.succ = reinterpret_cast<const uint4*>(succ);
-    if ((rc = t->upload(th.bits, &d.bits)) != NGAP_OK) return rc;
-    if ((rc = t->upload(th.rep, &d.rep)) != NGAP_OK) return rc;
+    d.ncls = th.ncls;
+    d.cw = th.cw;
+    d.kb = th.kb;
+    d.image_bytes = (int32_t)th.image.size();
+    d.off_cmask = th.off_cmask;
+    d.off_rep = th.off_rep;
+    d.off_cls = th.off_cls;
+    d.inj_batch = th.inj_batch;
+    if ((rc = t->upload(th.image, &d.image)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.sid, &d.sid)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.aas, &d.aas)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.start, &d.start)) != NGAP_OK) return rc;
@@ -189,6 +198,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       pd.nkeys = (int32_t)ph.keys.size();
       pd.nrkeys = (int32_t)ph.rkeys.size();
       pd.cutoff = ph.cutoff;
+      pd.has_reports = ph.rlist.empty() ? 0 : 1;
       if ((rc = t->upload(ph.keys, &pd.keys)) != NGAP_OK) return rc;
       if ((rc = t->upload(ph.voff, &pd.voff)) != NGAP_OK) return rc;
       if ((rc = t->upload(ph.vlist, &pd.vlist)) != NGAP_OK) return rc;
@@ -197,7 +207,9 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       if ((rc = t->upload(ph.rlist, &pd.rlist)) != NGAP_OK) return rc;
     }
     t->dev_desc.push_back(d);
+    if (d.image_bytes <= to.image_budget) t->image_region = std::max(t->image_region, d.image_bytes);
   }
+  t->image_region = (t->image_region + 127) & ~127;
   const TileDev* dt = nullptr;
   if ((rc = t->upload(t->dev_desc, &dt)) != NGAP_OK) return rc;
   t->d_tiles = const_cast<TileDev*>(dt);
@@ -288,9 +300,14 @@ int ensure_slots(ngap_engine* e, size_t slots, int max_states) {
 
 // Splits the work into units: unbounded tiles get one unit per segment;
 // bounded tiles are cut into chunks of `chunk` emitted positions, each with
-// max_path - 1 positions of warm-up (clamped at the segment start).
-void plan_units(const ngap_tables* t, const UnitPlanKey& k, std::vector<UnitDev>& units) {
+// max_path - 1 positions of warm-up (clamped at the segment start). Units of
+// one tile are then cut into CTA tasks: the long per-segment units of
+// unbounded tiles one per warp of a task and first, the chunks after them in
+// tasks sized to give every CTA several tasks.
+void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vector<UnitDev>& units,
+                std::vector<TaskDev>& tasks) {
   units.clear();
+  tasks.clear();
   std::vector<UnitDev> bounded;
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
     const TileHost& th = t->tiles[ti];
@@ -324,7 +341,26 @@ void plan_units(const ngap_tables* t, const UnitPlanKey& k, std::vector<UnitDev>
       }
     }
   }
+  const size_t nunb = units.size();
   units.insert(units.end(), bounded.begin(), bounded.end());
+  const int64_t per_b = std::max<int64_t>(
+      kWarpsPerCta, std::min<int64_t>(512, (int64_t)bounded.size() / std::max(1, 4 * grid)));
+  auto cut = [&](size_t b, size_t e, int64_t per) {
+    size_t i = b;
+    while (i < e) {
+      size_t j = i;
+      while (j < e && units[j].tile == units[i].tile && (int64_t)(j - i) < per) j++;
+      TaskDev tk;
+      tk.tile = units[i].tile;
+      tk.ubegin = (int32_t)i;
+      tk.uend = (int32_t)j;
+      tk.pad = 0;
+      tasks.push_back(tk);
+      i = j;
+    }
+  };
+  cut(0, nunb, kWarpsPerCta);
+  cut(nunb, units.size(), per_b);
 }
 
 __global__ void swap_halves(uint64_t* a, uint64_t n) {
@@ -425,7 +461,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   e->launches = 0;
   e->ran = false;
   int algo = p->algorithm;
-  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 2048;
+  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 1024;
   int table_depth = 0;
   for (auto& th : t->tiles) table_depth = std::max(table_depth, th.depth);
   switch (algo) {
@@ -453,11 +489,20 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   uint64_t cap = p->result_capacity > 0 ? p->result_capacity : 54619400ull;
   int rc = ensure_reports(e, cap);
   if (rc != NGAP_OK) return rc;
-  // units
+  // shared memory: the largest tile image that fits the budget, plus the warps
+  const int smem = cta_smem_bytes(window, t->image_region);
+  if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
+  int bps = 0;
+  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
+                                                              : blocks_per_sm<2>(smem, &bps);
+  if (rc != NGAP_OK) return rc;
+  const int full_grid = e->num_sms * bps;
+  // units and tasks
   UnitPlanKey key{p->num_seg, p->seg_len, p->is_dup ? 1 : 0, window, p->chunk, p->first_segment};
   if (e->plan_tables != t || key < e->plan_key || e->plan_key < key) {
     std::vector<UnitDev> units;
-    plan_units(t, key, units);
+    std::vector<TaskDev> tasks;
+    plan_units(t, key, full_grid, units, tasks);
     if (units.size() > e->units_cap) {
       cudaFree(e->d_units);
       e->d_units = nullptr;
@@ -465,22 +510,25 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
       CUDA_TRY(cudaMalloc(&e->d_units, units.size() * sizeof(UnitDev)));
       e->units_cap = units.size();
     }
+    if (tasks.size() > e->tasks_cap) {
+      cudaFree(e->d_tasks);
+      e->d_tasks = nullptr;
+      e->tasks_cap = 0;
+      CUDA_TRY(cudaMalloc(&e->d_tasks, tasks.size() * sizeof(TaskDev)));
+      e->tasks_cap = tasks.size();
+    }
     if (!units.empty())
       CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
                           cudaMemcpyHostToDevice));
+    if (!tasks.empty())
+      CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
+                          cudaMemcpyHostToDevice));
     e->nunits = (int32_t)units.size();
+    e->ntasks = (int32_t)tasks.size();
     e->plan_tables = t;
     e->plan_key = key;
   }
-  const int smem = kWarpsPerCta * warp_smem_bytes(window);
-  if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
-  int bps = 0;
-  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
-                                                              : blocks_per_sm<2>(smem, &bps);
-  if (rc != NGAP_OK) return rc;
-  int grid = e->num_sms * bps;
-  int need_blocks = (e->nunits + kWarpsPerCta - 1) / kWarpsPerCta;
-  grid = std::max(1, std::min(grid, need_blocks));
+  const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
   rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states);
   if (rc != NGAP_OK) return rc;
@@ -497,7 +545,9 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   MatchParams mp;
   mp.tiles = t->d_tiles;
   mp.units = e->d_units;
-  mp.nunits = e->nunits;
+  mp.tasks = e->d_tasks;
+  mp.ntasks = e->ntasks;
+  mp.image_region = t->image_region;
   mp.input = e->d_input;
   mp.window = window;
   mp.depth = depth;
@@ -508,7 +558,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.reports = e->d_reports;
   mp.rep_cap = cap;
   mp.err = e->d_err;
-  mp.unit_counter = e->d_unit_counter;
+  mp.task_counter = e->d_unit_counter;
   mp.carry = e->d_carry;
   mp.marks = e->d_marks;
   mp.ovf = e->d_ovf;
@@ -517,7 +567,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.ovf_cap = e->ovf_cap;
   mp.work = e->d_counters + 2;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
-  if (e->nunits > 0) {
+  if (e->ntasks > 0) {
     if (priv == 0) rc = launch_match<0>(e, mp, smem, st);
     else if (priv == 1) rc = launch_match<1>(e, mp, smem, st);
     else rc = launch_match<2>(e, mp, smem, st);

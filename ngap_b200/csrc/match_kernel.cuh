@@ -8,18 +8,26 @@
 // report state and creates entry (u, q + 1). Always-active states enter at
 // every position, either by scanning the always-active list (depth 0,
 // kernel_ngap_OA.cu:227-241) or through the prefix tables: the table of depth
-// k maps input[q .. q+k) to the states reached at q + k - 1 and, per depth, to
-// the reports at q .. q+k-1 (ngap.cu:2358-2513, kernel_ngap_OA.cu:242-311).
+// k maps the next k input symbols to the states reached at q + k - 1 and, per
+// depth, to the reports at q .. q+k-1 (ngap.cu:2358-2513,
+// kernel_ngap_OA.cu:242-311).
 //
-// B200 organisation (not the reference's): one warp per unit (a tile of CCs
-// over a range of positions), many warps per SM, no block-wide barrier in the
-// hot loop. Per warp, in shared memory: a LIFO worklist of packed entries
-// (state << 13 | offset in the window) pushed with ballot/popc aggregation and
-// spilling to a per-warp global overflow stack; a double-buffered input window
-// filled by cp.async.bulk (TMA 1-D copy, completion on an mbarrier, bounded
-// wait); a report buffer flushed with one global atomic per flush. Entries that
-// fall on the first position of the next window are carried over with exact
-// deduplication through a per-warp bitmap.
+// B200 organisation (not the reference's):
+//  * a CTA takes a task (a tile and a range of its units) and stages the
+//    tile's table image (successors, byte-class masks, report bits, byte ->
+//    class map) into shared memory once; its 16 warps then take units of that
+//    task, one warp per unit, with no block-wide barrier in the hot loop;
+//  * per warp, in shared memory: a LIFO worklist of packed entries
+//    (state << 13 | offset in the window); one expansion step pops up to 32
+//    entries, evaluates all their successors, and pushes the survivors with a
+//    single bit-sliced ballot prefix sum; entries past the shared capacity
+//    spill to a per-warp global overflow stack;
+//  * input windows are fetched by cp.async.bulk (1-D TMA, completion on an
+//    mbarrier, bounded wait), double-buffered, and translated to class ids in
+//    place;
+//  * reports go through a per-warp shared buffer flushed with one global atomic;
+//    states that land on the next window's first position are carried over
+//    with exact deduplication through a per-warp bitmap.
 #pragma once
 
 #include <cstdint>
@@ -28,13 +36,14 @@
 
 namespace ngap {
 
-constexpr int kWarpsPerCta = 8;
+constexpr int kWarpsPerCta = 16;
 constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr int kStackCap = 1024;   // entries per warp in shared memory
 constexpr int kReportBuf = 64;    // reports per warp buffered in shared memory
 constexpr int kInjectLow = 256;   // inject new positions while the stack holds fewer entries
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNoEntry = 0xffffffffu;  // never a valid entry: offsets stay < 8191
+constexpr uint32_t kIdMask = 0x7fffffffu;
 
 // Error flags written by the kernel (bit set => condition happened).
 constexpr int kErrQueue = 1;      // overflow stack full: results incomplete
@@ -45,7 +54,9 @@ constexpr int kErrCarry = 8;      // carry buffer full
 struct MatchParams {
   const TileDev* tiles;
   const UnitDev* units;
-  int32_t nunits;
+  const TaskDev* tasks;
+  int32_t ntasks;
+  int32_t image_region;     // shared-memory bytes reserved for a tile image
   const uint8_t* input;     // 16-byte aligned, readable up to round_up(len, 16)
   int32_t window;           // W <= kMaxWindow
   int32_t depth;            // 0: scan the AAS list; >= 1: tables up to min(depth, tile.depth)
@@ -56,7 +67,7 @@ struct MatchParams {
   uint64_t* reports;        // key = offset << 32 | id
   uint64_t rep_cap;
   int* err;
-  unsigned int* unit_counter;
+  unsigned int* task_counter;
   uint32_t* carry;          // [slots][carry_cap]
   uint32_t* marks;          // [slots][mark_words]
   uint32_t* ovf;            // [slots][ovf_cap]
@@ -68,6 +79,10 @@ __host__ __device__ inline int window_buf_bytes(int W) { return ((W + 48) + 15) 
 
 __host__ __device__ inline int warp_smem_bytes(int W) {
   return kStackCap * 4 + 2 * window_buf_bytes(W) + kReportBuf * 8 + 3 * 32 * 4 + 16;
+}
+
+__host__ __device__ inline int cta_smem_bytes(int W, int image_region) {
+  return image_region + kWarpsPerCta * warp_smem_bytes(W);
 }
 
 struct WarpSmem {
@@ -89,13 +104,23 @@ struct WarpRun {
   uint32_t* marks;
 };
 
-// Everything a warp needs about its current unit and window.
-struct UnitCtx {
+// The tile a warp works on: hot tables in shared memory (or global memory
+// when the image does not fit) and the cold ones in global memory.
+struct TileView {
+  const uint4* succ;
+  const uint32_t* cmask;
+  const uint32_t* rep;
+  const uint8_t* cls;
   const TileDev* t;
-  const uint8_t* in;  // window bytes: in[0] = input[wb]
+  int cw, kb;
+  uint32_t gbits;
+};
+
+// Everything about the current unit and window.
+struct UnitCtx {
+  const uint8_t* in;  // window symbols (class ids): in[0] = symbol at wb
   int64_t wb, hi, emit_lo;
   int wlen;
-  uint32_t gbits;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -136,15 +161,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ bool accepts(const uint32_t* __restrict__ bits, uint32_t v, uint32_t s) {
-  return (__ldg(bits + (size_t)v * 8 + (s >> 5)) >> (s & 31)) & 1u;
+__device__ __forceinline__ bool accepts(const TileView& tv, uint32_t v, uint32_t c) {
+  return (tv.cmask[(size_t)v * tv.cw + (c >> 5)] >> (c & 31)) & 1u;
 }
 
-__device__ __forceinline__ bool is_report(const uint32_t* __restrict__ rep, uint32_t v) {
-  return (__ldg(rep + (v >> 5)) >> (v & 31)) & 1u;
+__device__ __forceinline__ bool is_report(const TileView& tv, uint32_t v) {
+  return (tv.rep[v >> 5] >> (v & 31)) & 1u;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// Exclusive prefix sum over the warp of counts < 2^B, one ballot per bit.
+template <int B>
+__device__ __forceinline__ int warp_excl(int cnt, int lane, int& total) {
+  int ex = 0;
+  total = 0;
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const unsigned m = __ballot_sync(kFull, (cnt >> b) & 1);
+    ex += __popc(m & lanemask_lt(lane)) << b;
+    total += __popc(m) << b;
+  }
+  return ex;
+}
 
 __device__ __forceinline__ void flush_reports(const MatchParams& p, WarpSmem& ws, WarpRun& w, int lane) {
   if (w.nrep == 0) return;
@@ -153,7 +192,7 @@ __device__ __forceinline__ void flush_reports(const MatchParams& p, WarpSmem& ws
   base = __shfl_sync(kFull, base, 0);
   if (!p.report_off) {
     for (int i = lane; i < w.nrep; i += 32) {
-      unsigned long long idx = base + (unsigned long long)i;
+      const unsigned long long idx = base + (unsigned long long)i;
       if (idx < p.rep_cap) p.reports[idx] = ws.rbuf[i];
     }
     if (lane == 0 && base + (unsigned long long)w.nrep > p.rep_cap) atomicOr(p.err, kErrResults);
@@ -165,9 +204,9 @@ __device__ __forceinline__ void flush_reports(const MatchParams& p, WarpSmem& ws
 // Warp-aggregated report emission: lanes with pred append (offset, id).
 __device__ __forceinline__ void emit_report(const MatchParams& p, WarpSmem& ws, WarpRun& w, int lane,
                                             bool pred, uint32_t id, uint32_t off) {
-  unsigned m = __ballot_sync(kFull, pred);
+  const unsigned m = __ballot_sync(kFull, pred);
   if (m == 0) return;
-  int cnt = __popc(m);
+  const int cnt = __popc(m);
   if (w.nrep + cnt > kReportBuf) flush_reports(p, ws, w, lane);
   if (pred) ws.rbuf[w.nrep + __popc(m & lanemask_lt(lane))] = ((unsigned long long)off << 32) | id;
   w.nrep += cnt;
@@ -180,7 +219,7 @@ __device__ __forceinline__ void store_entry(const MatchParams& p, WarpSmem& ws, 
   if (i < kStackCap) {
     ws.stack[i] = e;
   } else {
-    int j = w.ovf_n + (i - kStackCap);
+    const int j = w.ovf_n + (i - kStackCap);
     if (j < p.ovf_cap) w.ovf[j] = e;
     else atomicOr(p.err, kErrQueue);
   }
@@ -198,7 +237,7 @@ __device__ __forceinline__ void grow_stack(const MatchParams& p, WarpRun& w, int
 // Warp-aggregated push of one entry per predicated lane.
 __device__ __forceinline__ void push_entry(const MatchParams& p, WarpSmem& ws, WarpRun& w, int lane,
                                            bool pred, uint32_t e) {
-  unsigned m = __ballot_sync(kFull, pred);
+  const unsigned m = __ballot_sync(kFull, pred);
   if (m == 0) return;
   if (pred) store_entry(p, ws, w, w.top + __popc(m & lanemask_lt(lane)), e);
   grow_stack(p, w, __popc(m));
@@ -210,13 +249,13 @@ __device__ __forceinline__ void carry_state(const MatchParams& p, WarpRun& w, in
                                             uint32_t u) {
   bool fresh = false;
   if (pred) {
-    uint32_t bit = 1u << (u & 31);
+    const uint32_t bit = 1u << (u & 31);
     fresh = !(atomicOr(w.marks + (u >> 5), bit) & bit);
   }
-  unsigned m = __ballot_sync(kFull, fresh);
+  const unsigned m = __ballot_sync(kFull, fresh);
   if (m == 0) return;
   if (fresh) {
-    int i = w.ncarry + __popc(m & lanemask_lt(lane));
+    const int i = w.ncarry + __popc(m & lanemask_lt(lane));
     if (i < p.carry_cap) w.carry[i] = u;
     else atomicOr(p.err, kErrCarry);
   }
@@ -237,8 +276,8 @@ __device__ __forceinline__ void pt_lookup(const PrefixTableDev& t, uint32_t key,
   int lo = 0, hi = (reports ? t.nrkeys : t.nkeys) - 1;
   b = e = 0;
   while (lo <= hi) {
-    int mid = (lo + hi) >> 1;
-    uint32_t k = __ldg(keys + mid);
+    const int mid = (lo + hi) >> 1;
+    const uint32_t k = __ldg(keys + mid);
     if (k == key) {
       b = __ldg(off + mid);
       e = __ldg(off + mid + 1);
@@ -249,55 +288,21 @@ __device__ __forceinline__ void pt_lookup(const PrefixTableDev& t, uint32_t key,
   }
 }
 
-// Handles a state u (bit 31 = report flag) that matched at window offset r,
-// 1 <= r <= wlen: report it, then push it (r < wlen), carry it (r == wlen), or
-// with privatization expand it in registers. Warp-collective: every lane
-// calls it with the same LEVEL and privatize.
-template <int LEVEL>
-__device__ __forceinline__ void handle_match(const MatchParams& p, WarpSmem& ws, WarpRun& w,
-                                             const UnitCtx& c, int lane, bool pred, uint32_t u,
-                                             int r, bool privatize) {
-  const int64_t q = c.wb + r;
-  const bool rep = pred && (u >> 31) && q >= c.emit_lo;
-  u &= 0x7fffffffu;
-  emit_report(p, ws, w, lane, rep, rep ? (__ldg(c.t->sid + u) | c.gbits) : 0u, (uint32_t)q);
-  const bool has_next = pred && q + 1 < c.hi;
-  if (LEVEL > 0 && privatize) {
-    const bool inner = has_next && r < c.wlen;
-    carry_state(p, w, lane, has_next && !inner, u);
-    uint4 sc = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
-    uint32_t s = 0;
-    if (inner) {
-      sc = __ldg(c.t->succ + u);
-      s = c.in[r + 1];
-    }
-    const uint32_t cs[4] = {sc.x, sc.y, sc.z, sc.w};
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const bool ok = inner && cs[j] != kNoSucc && accepts(c.t->bits, cs[j] & 0x7fffffffu, s);
-      handle_match<(LEVEL > 0 ? LEVEL - 1 : 0)>(p, ws, w, c, lane, ok, cs[j], r + 1, privatize);
-    }
-    return;
-  }
-  carry_state(p, w, lane, has_next && r == c.wlen, u);
-  push_entry(p, ws, w, lane, has_next && r < c.wlen, (u << kEntryPosBits) | (uint32_t)r);
-}
-
-// Always-active states for window offsets [r0, r0 + 32) (one per lane).
+// Always-active states for window offsets [r0, r0 + batch) (one per lane).
 __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpRun& w,
-                                       const UnitCtx& c, int lane, int r0, int depth,
-                                       unsigned long long& n_injected) {
-  const TileDev& t = *c.t;
+                                       const TileView& tv, const UnitCtx& c, int lane, int r0,
+                                       int batch, int depth, unsigned long long& n_injected) {
+  const TileDev& t = *tv.t;
   const int r = r0 + lane;
-  const bool valid = r < c.wlen;
+  const bool valid = lane < batch && r < c.wlen;
   const int64_t q = c.wb + r;
   if (depth == 0) {  // scan the always-active list
     const uint32_t s = valid ? c.in[r] : 0u;
     for (int i = 0; i < t.naas; i++) {
       const uint32_t a = __ldg(t.aas + i);
-      const bool ok = valid && accepts(t.bits, a, s);
-      const bool rep = ok && is_report(t.rep, a) && q >= c.emit_lo;
-      emit_report(p, ws, w, lane, rep, rep ? (__ldg(t.sid + a) | c.gbits) : 0u, (uint32_t)q);
+      const bool ok = valid && accepts(tv, a, s);
+      const bool rep = ok && is_report(tv, a) && q >= c.emit_lo;
+      emit_report(p, ws, w, lane, rep, rep ? (__ldg(t.sid + a) | tv.gbits) : 0u, (uint32_t)q);
       push_entry(p, ws, w, lane, ok && q + 1 < c.hi, (a << kEntryPosBits) | (uint32_t)r);
       n_injected += ok;
     }
@@ -308,15 +313,17 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
   uint32_t key = 0, vb = 0, ve = 0;
   for (int d = 0; d < depth; d++) {
     const bool act = d < k;
-    if (act) key = (key << 8) | c.in[r + d];
-    uint32_t rb = 0, re = 0;
-    if (act) pt_lookup(t.pt[d], key, true, rb, re);
-    const int len = (int)(re - rb);
-    const int mx = __reduce_max_sync(kFull, len);
-    for (int i = 0; i < mx; i++) {
-      const bool ok = i < len && q + d >= c.emit_lo;
-      const uint32_t v = ok ? __ldg(t.pt[d].rlist + rb + i) : 0u;
-      emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v) | c.gbits) : 0u, (uint32_t)(q + d));
+    if (act) key = (key << tv.kb) | c.in[r + d];
+    if (t.pt[d].has_reports) {
+      uint32_t rb = 0, re = 0;
+      if (act) pt_lookup(t.pt[d], key, true, rb, re);
+      const int len = (int)(re - rb);
+      const int mx = __reduce_max_sync(kFull, len);
+      for (int i = 0; i < mx; i++) {
+        const bool ok = i < len && q + d >= c.emit_lo;
+        const uint32_t v = ok ? __ldg(t.pt[d].rlist + rb + i) : 0u;
+        emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v) | tv.gbits) : 0u, (uint32_t)(q + d));
+      }
     }
     if (act && d == k - 1) pt_lookup(t.pt[d], key, false, vb, ve);
   }
@@ -326,7 +333,7 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
   uint32_t incl = len;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(kFull, incl, o);
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
     if (lane >= o) incl += y;
   }
   const uint32_t total = __shfl_sync(kFull, incl, 31);
@@ -352,12 +359,136 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
   __syncwarp();
 }
 
+// Reports (slow path, taken only when some lane has one) for up to 4 matched
+// states u[j] (bit 31 = report flag) at stream position q.
+__device__ __forceinline__ void report4(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                        const TileView& tv, int lane, const bool ok[4],
+                                        const uint32_t u[4], int64_t q, bool in_range) {
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < 4; j++) any |= ok[j] && (u[j] >> 31);
+  if (!__any_sync(kFull, any && in_range)) return;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const bool rep = in_range && ok[j] && (u[j] >> 31);
+    emit_report(p, ws, w, lane, rep, rep ? (__ldg(tv.t->sid + (u[j] & kIdMask)) | tv.gbits) : 0u,
+                (uint32_t)q);
+  }
+}
+
+// Expands the up-to-32 entries on top of the stack: one step of the worklist.
 template <int PRIV>
-__global__ void __launch_bounds__(kCtaThreads) match_kernel(MatchParams p) {
+__device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                            const TileView& tv, const UnitCtx& c, int lane,
+                                            unsigned long long& n_expanded) {
+  const int n = min(w.top, 32);
+  uint32_t e = lane < n ? ws.stack[w.top - 1 - lane] : kNoEntry;
+  w.top -= n;
+  __syncwarp();
+  if (p.unique) {  // identical entries in one step are expanded once (--unique)
+    const unsigned peers = __match_any_sync(kFull, e);
+    if ((__ffs(peers) - 1) != lane) e = kNoEntry;
+  }
+  const uint32_t v = e >> kEntryPosBits;
+  const int r = (int)(e & ((1u << kEntryPosBits) - 1));
+  const int64_t q = c.wb + r;
+  const bool go = e != kNoEntry && q + 1 < c.hi;
+  uint4 sc = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+  uint32_t s = 0;
+  if (go) {
+    sc = tv.succ[v];
+    s = c.in[r + 1];
+  }
+  n_expanded += go;
+  const uint32_t u[4] = {sc.x, sc.y, sc.z, sc.w};
+  bool ok[4];
+  int cnt = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    ok[j] = go && u[j] != kNoSucc && accepts(tv, u[j] & kIdMask, s);
+    cnt += ok[j];
+  }
+  report4(p, ws, w, tv, lane, ok, u, q + 1, q + 1 >= c.emit_lo);
+  const bool need = go && q + 2 < c.hi;        // the successors have a next symbol
+  const bool at_end = r + 1 == c.wlen;         // successors sit at the next window's start
+  if (__any_sync(kFull, need && at_end)) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) carry_state(p, w, lane, need && at_end && ok[j], u[j] & kIdMask);
+  }
+  const bool privatize =
+      PRIV > 0 && __popc(__ballot_sync(kFull, go)) > p.active_threshold;
+  if (!privatize) {
+    const int pc = (need && !at_end) ? cnt : 0;
+    int total;
+    const int ex = warp_excl<3>(pc, lane, total);
+    if (pc) {
+      int pos = w.top + ex;
+      const uint32_t tag = (uint32_t)(r + 1);
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (ok[j]) store_entry(p, ws, w, pos++, ((u[j] & kIdMask) << kEntryPosBits) | tag);
+    }
+    grow_stack(p, w, total);
+    __syncwarp();
+    return;
+  }
+  // privatization (kernel_ngap_OA.cu:96-138): expand the matched successors in
+  // registers one more level instead of pushing them
+  const bool inner = need && !at_end;  // successors' successors read in[r + 2] <= window end
+  const uint32_t s2 = inner ? c.in[r + 2] : 0u;
+  uint32_t u2[4][4];
+  bool ok2[4][4];
+  int cnt2 = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    uint4 sc2 = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+    if (inner && ok[j]) sc2 = tv.succ[u[j] & kIdMask];
+    u2[j][0] = sc2.x;
+    u2[j][1] = sc2.y;
+    u2[j][2] = sc2.z;
+    u2[j][3] = sc2.w;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      ok2[j][k] = u2[j][k] != kNoSucc && accepts(tv, u2[j][k] & kIdMask, s2);
+      cnt2 += ok2[j][k];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) report4(p, ws, w, tv, lane, ok2[j], u2[j], q + 2, q + 2 >= c.emit_lo);
+  const bool need2 = inner && q + 3 < c.hi;
+  const bool at_end2 = r + 2 == c.wlen;
+  if (__any_sync(kFull, need2 && at_end2)) {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        carry_state(p, w, lane, need2 && at_end2 && ok2[j][k], u2[j][k] & kIdMask);
+  }
+  const int pc = (need2 && !at_end2) ? cnt2 : 0;
+  int total;
+  const int ex = warp_excl<5>(pc, lane, total);
+  if (pc) {
+    int pos = w.top + ex;
+    const uint32_t tag = (uint32_t)(r + 2);
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (ok2[j][k]) store_entry(p, ws, w, pos++, ((u2[j][k] & kIdMask) << kEntryPosBits) | tag);
+  }
+  grow_stack(p, w, total);
+  __syncwarp();
+}
+
+template <int PRIV>
+__global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
+  __shared__ int s_task;
+  __shared__ unsigned s_next;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = p.window;
-  uint8_t* base = smem_raw + (size_t)warp * warp_smem_bytes(W);
+  uint8_t* image = smem_raw;
+  uint8_t* base = smem_raw + p.image_region + (size_t)warp * warp_smem_bytes(W);
   WarpSmem ws;
   ws.stack = reinterpret_cast<uint32_t*>(base);
   ws.in[0] = base + kStackCap * 4;
@@ -381,6 +512,7 @@ __global__ void __launch_bounds__(kCtaThreads) match_kernel(MatchParams p) {
   bool pending[2] = {false, false};
   bool dead = false;
   unsigned long long n_expanded = 0, n_injected = 0;
+  int staged = -1;  // tile whose image is in shared memory
 
   auto issue = [&](int buf, int64_t wb, int64_t hi) {
     const int64_t we = min(wb + (int64_t)W, hi);
@@ -392,122 +524,130 @@ __global__ void __launch_bounds__(kCtaThreads) match_kernel(MatchParams p) {
       bulk_g2s(ws.in[buf], p.input + a0, bytes, &ws.bar[buf]);
     }
     pending[buf] = true;
+    return bytes;
   };
 
-  while (!dead) {
-    unsigned uid = 0;
-    if (lane == 0) uid = atomicAdd(p.unit_counter, 1u);
-    uid = __shfl_sync(kFull, uid, 0);
-    if (uid >= (unsigned)p.nunits) break;
-    const UnitDev un = p.units[uid];
-    UnitCtx c;
-    c.t = &p.tiles[un.tile];
-    c.hi = un.hi;
-    c.emit_lo = un.emit_lo;
-    c.gbits = (uint32_t)c.t->group << 22;
-    const int depth = p.depth == 0 ? 0 : min(p.depth, c.t->depth);
-    int cur = 0;
-    issue(0, un.lo, c.hi);
-    for (int64_t wb = un.lo; wb < c.hi; wb += W) {
-      const int64_t we = min(wb + (int64_t)W, c.hi);
-      c.wb = wb;
-      c.wlen = (int)(we - wb);
-      if (!mbar_wait(&ws.bar[cur], phase[cur])) {
-        if (lane == 0) atomicOr(p.err, kErrTimeout);
-        dead = true;
-        break;
-      }
-      phase[cur] ^= 1u;
-      pending[cur] = false;
-      if (we < c.hi) issue(cur ^ 1, we, c.hi);
-      c.in = ws.in[cur] + (wb & 15);
-      __syncwarp();
-      // carried states: matched at wb
-      w.top = 0;
-      if (w.ncarry > 0) {
-        for (int i = lane; i < w.ncarry; i += 32) {
-          const uint32_t u = w.carry[i];
-          w.marks[u >> 5] = 0u;
-          store_entry(p, ws, w, i, u << kEntryPosBits);
-        }
-        const int n = w.ncarry;
-        w.ncarry = 0;
-        grow_stack(p, w, n);
-        __syncwarp();
-      }
-      // start-of-data states at the unit's first position (ngap_buffer.cu:613-631)
-      if (wb == un.lo && (un.flags & 1u)) {
-        const uint32_t s0 = c.in[0];
-        for (int i0 = 0; i0 < c.t->nstart; i0 += 32) {
-          const int i = i0 + lane;
-          const uint32_t v = i < c.t->nstart ? __ldg(c.t->start + i) : 0u;
-          const bool ok = i < c.t->nstart && accepts(c.t->bits, v, s0);
-          const bool rep = ok && is_report(c.t->rep, v) && un.lo >= c.emit_lo;
-          emit_report(p, ws, w, lane, rep, rep ? (__ldg(c.t->sid + v) | c.gbits) : 0u,
-                      (uint32_t)un.lo);
-          push_entry(p, ws, w, lane, ok && un.lo + 1 < c.hi, v << kEntryPosBits);
-        }
-      }
-      int cursor = 0;  // next window offset to inject
-      while (true) {
-        if (w.top < kInjectLow && cursor < c.wlen) {
-          inject(p, ws, w, c, lane, cursor, depth, n_injected);
-          cursor += 32;
-          continue;
-        }
-        if (w.top == 0) {
-          if (w.ovf_n > 0) {  // refill from the overflow stack
-            const int m = min(w.ovf_n, kStackCap);
-            for (int i = lane; i < m; i += 32) ws.stack[i] = w.ovf[w.ovf_n - m + i];
-            w.ovf_n -= m;
-            w.top = m;
-            __syncwarp();
-            continue;
-          }
-          if (cursor < c.wlen) continue;
+  while (true) {
+    if (threadIdx.x == 0) s_task = (int)atomicAdd(p.task_counter, 1u);
+    __syncthreads();
+    const int task = s_task;
+    if (task >= p.ntasks) break;
+    const TaskDev tk = p.tasks[task];
+    const TileDev* t = &p.tiles[tk.tile];
+    const bool fits = t->image_bytes <= p.image_region;
+    if (fits && staged != tk.tile) {  // stage the tile image (all warps are past the last task)
+      const uint4* src = reinterpret_cast<const uint4*>(t->image);
+      uint4* dst = reinterpret_cast<uint4*>(image);
+      for (int i = threadIdx.x; i < t->image_bytes / 16; i += kCtaThreads) dst[i] = __ldg(src + i);
+      staged = tk.tile;
+    }
+    if (threadIdx.x == 0) s_next = (unsigned)tk.ubegin;
+    __syncthreads();
+    TileView tv;
+    const uint8_t* ib = fits ? image : t->image;
+    tv.succ = reinterpret_cast<const uint4*>(ib);
+    tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
+    tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
+    tv.cls = ib + t->off_cls;
+    tv.t = t;
+    tv.cw = t->cw;
+    tv.kb = t->kb;
+    tv.gbits = (uint32_t)t->group << 22;
+    const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
+    const int batch = depth == 0 ? 32 : t->inj_batch;
+    const bool translate = t->cw != 8;
+
+    while (!dead) {
+      unsigned uid = 0;
+      if (lane == 0) uid = atomicAdd(&s_next, 1u);
+      uid = __shfl_sync(kFull, uid, 0);
+      if (uid >= (unsigned)tk.uend) break;
+      const UnitDev un = p.units[uid];
+      UnitCtx c;
+      c.hi = un.hi;
+      c.emit_lo = un.emit_lo;
+      int cur = 0;
+      uint32_t nbytes[2];
+      nbytes[0] = issue(0, un.lo, c.hi);
+      for (int64_t wb = un.lo; wb < c.hi; wb += W) {
+        const int64_t we = min(wb + (int64_t)W, c.hi);
+        c.wb = wb;
+        c.wlen = (int)(we - wb);
+        if (!mbar_wait(&ws.bar[cur], phase[cur])) {
+          if (lane == 0) atomicOr(p.err, kErrTimeout);
+          dead = true;
           break;
         }
-        // expand up to 32 entries from the top of the stack
-        const int n = min(w.top, 32);
-        const bool has = lane < n;
-        uint32_t e = has ? ws.stack[w.top - 1 - lane] : kNoEntry;
-        w.top -= n;
+        phase[cur] ^= 1u;
+        pending[cur] = false;
+        if (translate) {  // bytes -> class ids, in place
+          for (uint32_t i = lane; i < nbytes[cur]; i += 32) ws.in[cur][i] = tv.cls[ws.in[cur][i]];
+        }
         __syncwarp();
-        if (p.unique) {  // identical entries in one step are expanded once (--unique)
-          const unsigned peers = __match_any_sync(kFull, e);
-          if ((__ffs(peers) - 1) != lane) e = kNoEntry;
+        if (we < c.hi) nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi);
+        c.in = ws.in[cur] + (wb & 15);
+        // carried states: matched at wb
+        w.top = 0;
+        if (w.ncarry > 0) {
+          for (int i = lane; i < w.ncarry; i += 32) {
+            const uint32_t u = w.carry[i];
+            w.marks[u >> 5] = 0u;
+            store_entry(p, ws, w, i, u << kEntryPosBits);
+          }
+          const int nc = w.ncarry;
+          w.ncarry = 0;
+          grow_stack(p, w, nc);
+          __syncwarp();
         }
-        const uint32_t v = e >> kEntryPosBits;
-        const int r = (int)(e & ((1u << kEntryPosBits) - 1));
-        const bool go = e != kNoEntry && c.wb + r + 1 < c.hi;
-        uint4 sc = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
-        uint32_t s = 0;
-        if (go) {
-          sc = __ldg(c.t->succ + v);
-          s = c.in[r + 1];
+        // start-of-data states at the unit's first position (ngap_buffer.cu:613-631)
+        if (wb == un.lo && (un.flags & 1u)) {
+          const uint32_t s0 = c.in[0];
+          for (int i0 = 0; i0 < t->nstart; i0 += 32) {
+            const int i = i0 + lane;
+            const uint32_t v = i < t->nstart ? __ldg(t->start + i) : 0u;
+            const bool ok = i < t->nstart && accepts(tv, v, s0);
+            const bool rep = ok && is_report(tv, v) && un.lo >= c.emit_lo;
+            emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v) | tv.gbits) : 0u,
+                        (uint32_t)un.lo);
+            push_entry(p, ws, w, lane, ok && un.lo + 1 < c.hi, v << kEntryPosBits);
+          }
         }
-        n_expanded += go;
-        const bool privatize = PRIV > 0 && __popc(__ballot_sync(kFull, go)) > p.active_threshold;
-        const uint32_t cs[4] = {sc.x, sc.y, sc.z, sc.w};
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const bool ok = go && cs[j] != kNoSucc && accepts(c.t->bits, cs[j] & 0x7fffffffu, s);
-          handle_match<PRIV>(p, ws, w, c, lane, ok, cs[j], r + 1, privatize);
+        int cursor = 0;  // next window offset to inject
+        while (true) {
+          if (w.top < kInjectLow && cursor < c.wlen) {
+            inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
+            cursor += batch;
+            continue;
+          }
+          if (w.top == 0) {
+            if (w.ovf_n > 0) {  // refill from the overflow stack
+              const int m = min(w.ovf_n, kStackCap);
+              for (int i = lane; i < m; i += 32) ws.stack[i] = w.ovf[w.ovf_n - m + i];
+              w.ovf_n -= m;
+              w.top = m;
+              __syncwarp();
+              continue;
+            }
+            if (cursor < c.wlen) continue;
+            break;
+          }
+          expand_step<PRIV>(p, ws, w, tv, c, lane, n_expanded);
         }
+        cur ^= 1;
       }
-      cur ^= 1;
+      if (dead) {
+        for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;
+        w.ncarry = w.top = w.ovf_n = 0;
+        // wait (bounded) for any copy still in flight before giving up on this warp
+        for (int b = 0; b < 2; b++)
+          if (pending[b]) {
+            mbar_wait(&ws.bar[b], phase[b]);
+            pending[b] = false;
+          }
+        __syncwarp();
+      }
     }
-    if (dead) {
-      for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;
-      w.ncarry = w.top = w.ovf_n = 0;
-      // wait (bounded) for any copy still in flight before leaving
-      for (int b = 0; b < 2; b++)
-        if (pending[b]) {
-          mbar_wait(&ws.bar[b], phase[b]);
-          pending[b] = false;
-        }
-      __syncwarp();
-    }
+    __syncthreads();  // every warp is done with this task before the image is replaced
   }
   flush_reports(p, ws, w, lane);
 #pragma unroll

@@ -1,4 +1,4 @@
-// Tiles and prefix-memoization tables.
+// Tiles, byte classes, shared-memory images and prefix-memoization tables.
 //
 // A tile is a set of whole CCs of one group. CCs never share states or edges,
 // so splitting a group into tiles changes no report: a report keeps its
@@ -12,15 +12,23 @@
 //     such CCs can be matched in independent chunks with L-1 positions of
 //     warm-up, reports in the warm-up being left to the previous chunk.
 //
+// Byte classes: two bytes are equivalent for a tile when every state of the
+// tile accepts both or neither. With at most 32 (64) classes a state's symbol
+// class shrinks from 256 bits to one (two) words and the input is translated
+// to class ids once per window.
+//
 // Prefix tables follow ngap::getPrecomputeResultsForKGroupsInCsr and
 // recursivePrecomputeForK (code/src/ngap/ngap.cu:2358-2513): table 1 maps a
-// byte to the always-active states accepting it; table d maps a d-byte key to
-// the successors of table d-1's states accepting the last byte; each table also
-// lists the report states among its states. Lists are deduplicated (the
-// reference keeps duplicates; the set of activations is the same).
+// symbol to the always-active states accepting it; table d maps d symbols to
+// the successors of table d-1's states accepting the last symbol; each table
+// also lists the report states among its states. Here the symbols are byte
+// classes (the reference keys by bytes; the lists are the same for every byte
+// of a class), and lists are deduplicated (the reference keeps duplicates; the
+// set of activations is the same).
 #include "tables.h"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 
 namespace ngap {
@@ -62,18 +70,42 @@ int32_t cc_longest_path(const GroupGraph& g, int32_t b, int32_t e) {
   return m;
 }
 
-inline bool accepts(const TileHost& t, uint32_t v, int s) {
-  return (t.bits[(size_t)v * 8 + (s >> 5)] >> (s & 31)) & 1u;
+// Partition of the 256 bytes into classes, refined state by state; class ids
+// are numbered in order of their smallest byte.
+struct Partition {
+  uint16_t id[256];
+  int n = 1;
+  Partition() { memset(id, 0, sizeof(id)); }
+  void refine(const uint32_t* bits) {
+    int16_t map[512];
+    memset(map, -1, sizeof(map));
+    uint16_t nid[256];
+    int n2 = 0;
+    for (int b = 0; b < 256; b++) {
+      int k = id[b] * 2 + (int)((bits[b >> 5] >> (b & 31)) & 1u);
+      if (map[k] < 0) map[k] = (int16_t)n2++;
+      nid[b] = (uint16_t)map[k];
+    }
+    memcpy(id, nid, sizeof(id));
+    n = n2;
+  }
+};
+
+int class_words(int ncls) { return ncls <= 32 ? 1 : (ncls <= 64 ? 2 : 8); }
+
+inline bool accepts_cls(const TileHost& t, uint32_t v, int c) {
+  return (t.cmask[(size_t)v * t.cw + (c >> 5)] >> (c & 31)) & 1u;
 }
 
 inline bool is_report(const TileHost& t, uint32_t v) { return (t.rep[v >> 5] >> (v & 31)) & 1u; }
 
-void finish_table(PrefixTableHost& pt, int depth, const std::map<uint32_t, std::vector<uint32_t>>& lists,
-                  const TileHost& t, int cutoff_opt) {
-  pt.dense = depth <= 2;
-  uint64_t space = 1ull << (8 * depth);
+void finish_table(PrefixTableHost& pt, int key_bits,
+                  const std::map<uint32_t, std::vector<uint32_t>>& lists, const TileHost& t,
+                  int cutoff_opt) {
+  pt.dense = key_bits <= kDenseKeyBits;
   int64_t total = 0, nonzero = 0;
   if (pt.dense) {
+    const uint64_t space = 1ull << key_bits;
     pt.voff.assign(space + 1, 0);
     pt.roff.assign(space + 1, 0);
     std::vector<uint32_t> vcount(space, 0), rcount(space, 0);
@@ -124,16 +156,16 @@ void finish_table(PrefixTableHost& pt, int depth, const std::map<uint32_t, std::
 }
 
 void build_prefix_tables(TileHost& t, const TableOpts& opts) {
-  int want = std::max(1, std::min(opts.precompute_depth, kMaxDepth));
-  int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)8 << 20;
+  const int want = std::max(1, std::min(opts.precompute_depth, kMaxDepth));
+  const int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)4 << 20;
   std::map<uint32_t, std::vector<uint32_t>> prev, cur;
-  for (int s = 0; s < 256; s++) {
+  for (int c = 0; c < t.ncls; c++) {
     std::vector<uint32_t> l;
     for (uint32_t a : t.aas)
-      if (accepts(t, a, s)) l.push_back(a);
-    if (!l.empty()) prev[(uint32_t)s] = std::move(l);
+      if (accepts_cls(t, a, c)) l.push_back(a);
+    if (!l.empty()) prev[(uint32_t)c] = std::move(l);
   }
-  finish_table(t.pt[0], 1, prev, t, opts.precompute_cutoff);
+  finish_table(t.pt[0], t.kb, prev, t, opts.precompute_cutoff);
   t.depth = 1;
   std::vector<uint32_t> mark(t.nstates, 0);
   uint32_t stamp = 0;
@@ -142,7 +174,7 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
     int64_t total = 0;
     bool too_big = false;
     for (auto& kv : prev) {
-      for (int s = 0; s < 256 && !too_big; s++) {
+      for (int c = 0; c < t.ncls && !too_big; c++) {
         std::vector<uint32_t> l;
         stamp++;
         for (uint32_t v : kv.second) {
@@ -151,7 +183,7 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
             uint32_t u = sc[j];
             if (u == kNoSucc) continue;
             u &= 0x7fffffffu;
-            if (!accepts(t, u, s) || mark[u] == stamp) continue;
+            if (!accepts_cls(t, u, c) || mark[u] == stamp) continue;
             mark[u] = stamp;
             l.push_back(u);
           }
@@ -159,17 +191,40 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
         if (!l.empty()) {
           std::sort(l.begin(), l.end());
           total += (int64_t)l.size();
-          cur[(kv.first << 8) | (uint32_t)s] = std::move(l);
+          cur[(kv.first << t.kb) | (uint32_t)c] = std::move(l);
           if (total > cap) too_big = true;
         }
       }
       if (too_big) break;
     }
     if (too_big) break;
-    finish_table(t.pt[d - 1], d, cur, t, opts.precompute_cutoff);
+    finish_table(t.pt[d - 1], d * t.kb, cur, t, opts.precompute_cutoff);
     t.depth = d;
     prev.swap(cur);
   }
+  // positions injected per refill: keep one refill's lists within about half
+  // of a warp's shared worklist
+  const PrefixTableHost& deep = t.pt[t.depth - 1];
+  const int mean = std::max(1, deep.cutoff);
+  t.inj_batch = std::max(1, std::min(32, 512 / (mean + 1)));
+}
+
+void build_image(TileHost& t) {
+  auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  const size_t n = (size_t)t.nstates;
+  t.off_cmask = (int32_t)r16(n * 16);
+  t.off_rep = t.off_cmask + (int32_t)r16(n * t.cw * 4);
+  t.off_cls = t.off_rep + (int32_t)r16(((n + 31) / 32) * 4);
+  t.image.assign((size_t)t.off_cls + 256, 0);
+  memcpy(t.image.data(), t.succ.data(), n * 16);
+  memcpy(t.image.data() + t.off_cmask, t.cmask.data(), n * t.cw * 4);
+  memcpy(t.image.data() + t.off_rep, t.rep.data(), t.rep.size() * 4);
+  memcpy(t.image.data() + t.off_cls, t.cls.data(), 256);
+}
+
+int degree_error() {
+  set_error("internal error: a state has more than 4 successors after degree limiting");
+  return NGAP_E_INVALID;
 }
 
 bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, const TableOpts& opts,
@@ -180,30 +235,50 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   int32_t n = 0;
   bool bounded = true;
   int32_t mp = 0;
+  Partition part;
   for (auto& c : ccs) {
     n += c.end - c.begin;
     bounded = bounded && c.bounded;
     mp = std::max(mp, c.max_path);
+    for (int32_t v = c.begin; v < c.end; v++) part.refine(&g.bits[(size_t)v * 8]);
   }
   t.nstates = n;
   t.num_ccs = (int32_t)ccs.size();
   t.max_path = bounded ? mp : -1;
+  t.cw = class_words(part.n);
+  t.cls.resize(256);
+  if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
+    t.ncls = 256;
+    t.kb = 8;
+    for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)b;
+  } else {
+    t.ncls = part.n;
+    t.kb = t.cw == 1 ? 5 : 6;
+    for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)part.id[b];
+  }
   t.succ.assign((size_t)n * 4, kNoSucc);
   t.bits.resize((size_t)n * 8);
+  t.cmask.assign((size_t)n * t.cw, 0);
   t.rep.assign((n + 31) / 32, 0);
   t.sid.resize(n);
   int32_t local = 0;
   for (auto& c : ccs) {
     for (int32_t v = c.begin; v < c.end; v++, local++) {
       t.sid[local] = (uint32_t)v;
-      for (int w = 0; w < 8; w++) t.bits[(size_t)local * 8 + w] = g.bits[(size_t)v * 8 + w];
+      const uint32_t* bv = &g.bits[(size_t)v * 8];
+      for (int w = 0; w < 8; w++) t.bits[(size_t)local * 8 + w] = bv[w];
+      for (int b = 0; b < 256; b++)
+        if ((bv[b >> 5] >> (b & 31)) & 1u) {
+          int cl = t.cls[b];
+          t.cmask[(size_t)local * t.cw + (cl >> 5)] |= 1u << (cl & 31);
+        }
       if (g.attrs[v] & 2) t.rep[local >> 5] |= 1u << (local & 31);
       if (g.attrs[v] & 1) t.aas.push_back((uint32_t)local);
       int j = 0;
       for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
         int32_t u = g.cols[k];
         if (g.attrs[u] & 1) continue;  // redundant: u is active at every position
-        if (j >= 4) return false;  // the degree limiter guarantees at most 4
+        if (j >= 4) return false;      // the degree limiter guarantees at most 4
         uint32_t ul = (uint32_t)(u - c.begin + (local - (v - c.begin)));
         t.succ[(size_t)local * 4 + j++] = ul | ((g.attrs[u] & 2) ? 0x80000000u : 0u);
       }
@@ -221,24 +296,21 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
     }
   }
   build_prefix_tables(t, opts);
+  build_image(t);
   tiles.push_back(std::move(t));
   return true;
-}
-
-int degree_error() {
-  set_error("internal error: a state has more than 4 successors after degree limiting");
-  return NGAP_E_INVALID;
 }
 
 }  // namespace
 
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles) {
   tiles.clear();
-  const int32_t tile_states = opts.tile_states > 0 ? opts.tile_states : 2048;
+  const int64_t max_states = opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2;
   for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
     const GroupGraph& g = gs.groups[gi];
     std::vector<CcInfo> open[2];  // [0] bounded, [1] unbounded
     int32_t open_n[2] = {0, 0};
+    Partition open_part[2];
     const int nccs = (int)g.cc_begin.size() - 1;
     for (int c = 0; c < nccs; c++) {
       CcInfo ci;
@@ -247,12 +319,20 @@ int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>
       int32_t lp = cc_longest_path(g, ci.begin, ci.end);
       ci.bounded = lp >= 0 && lp <= opts.max_warmup;
       ci.max_path = ci.bounded ? lp : -1;
-      int k = ci.bounded ? 0 : 1;
-      int32_t sz = ci.end - ci.begin;
-      if (!open[k].empty() && open_n[k] + sz > tile_states) {
+      const int k = ci.bounded ? 0 : 1;
+      const int32_t sz = ci.end - ci.begin;
+      Partition trial = open_part[k];
+      for (int32_t v = ci.begin; v < ci.end; v++) trial.refine(&g.bits[(size_t)v * 8]);
+      const bool fits = open_n[k] + sz <= max_states &&
+                        image_bytes(open_n[k] + sz, class_words(trial.n)) <= opts.image_budget;
+      if (!open[k].empty() && !fits) {
         if (!emit_tile(g, gi, open[k], opts, tiles)) return degree_error();
         open[k].clear();
         open_n[k] = 0;
+        open_part[k] = Partition();
+        for (int32_t v = ci.begin; v < ci.end; v++) open_part[k].refine(&g.bits[(size_t)v * 8]);
+      } else {
+        open_part[k] = trial;
       }
       open[k].push_back(ci);
       open_n[k] += sz;

@@ -1,5 +1,5 @@
-// Host-side construction of the matching tables: tiles of CCs and their
-// prefix-memoization tables.
+// Host-side construction of the matching tables: tiles of CCs, their byte
+// classes, shared-memory images and prefix-memoization tables.
 #pragma once
 
 #include <vector>
@@ -14,7 +14,6 @@ struct PrefixTableHost {
   int32_t cutoff = 0;
   std::vector<uint32_t> keys, voff, vlist;
   std::vector<uint32_t> rkeys, roff, rlist;
-  int64_t entries() const { return (int64_t)vlist.size() + (int64_t)rlist.size(); }
 };
 
 struct TileHost {
@@ -23,21 +22,34 @@ struct TileHost {
   int32_t depth = 0;
   int32_t max_path = -1;
   int32_t num_ccs = 0;
-  std::vector<uint32_t> succ;  // nstates * 4
-  std::vector<uint32_t> bits;  // nstates * 8
-  std::vector<uint32_t> rep;   // ceil(nstates / 32)
-  std::vector<uint32_t> sid;   // nstates
+  int32_t ncls = 0, cw = 8, kb = 8;
+  int32_t inj_batch = 32;            // positions injected per worklist refill
+  std::vector<uint8_t> cls;          // 256: byte -> class
+  std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
+  std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
+  std::vector<uint32_t> cmask;       // nstates * cw
+  std::vector<uint32_t> rep;         // ceil(nstates / 32)
+  std::vector<uint32_t> sid;         // nstates
   std::vector<uint32_t> aas, start;
+  std::vector<uint8_t> image;        // succ | cmask | rep | cls, 16-byte aligned parts
+  int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
   PrefixTableHost pt[kMaxDepth];
 };
 
 struct TableOpts {
   int precompute_depth = 0;
   int precompute_cutoff = -1;
-  int tile_states = 0;              // 0 = automatic
+  int tile_states = 0;              // max states per tile; 0 = fill the image budget
   int64_t max_table_entries = 0;    // 0 = automatic
+  int image_budget = 96 * 1024;     // bytes of shared memory for one tile's image
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
 };
+
+// Bytes of a tile image with n states and cw class words.
+inline int64_t image_bytes(int64_t n, int cw) {
+  auto r16 = [](int64_t x) { return (x + 15) & ~(int64_t)15; };
+  return r16(n * 16) + r16(n * cw * 4) + r16(((n + 31) / 32) * 4) + 256;
+}
 
 // Splits every group into tiles and builds each tile's tables.
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles);
