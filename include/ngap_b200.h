@@ -99,7 +99,10 @@ void ngap_groups_destroy(ngap_groups* g);
 
 typedef struct ngap_table_opts {
   int device;            /* CUDA device ordinal */
-  int precompute_depth;  /* --precompute-depth 0..3: prefix-memoization depth */
+  int precompute_depth;  /* --precompute-depth: prefix-memoization depth 0..8 (the
+                            reference allows 0..3; keys are byte-class ids, so
+                            deeper tables stay small); -1 = as deep as the size
+                            caps allow */
   int precompute_cutoff; /* --precompute-cutoff, -1 = mean list length (precompute_table.cu:171) */
   int tile_states;       /* max states per tile; 0 = automatic */
   int64_t max_table_entries; /* cap on prefix-table list entries per tile; 0 = automatic */

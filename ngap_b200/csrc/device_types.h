@@ -8,16 +8,17 @@
 namespace ngap {
 
 constexpr uint32_t kNoSucc = 0xffffffffu;
-constexpr int kMaxDepth = 3;         // prefix-memoization depth limit (reference: 0..3)
+constexpr int kMaxDepth = 8;         // prefix-memoization depth limit (the reference stops at 3)
 constexpr int kEntryPosBits = 13;    // worklist entry = local_state << 13 | window offset
 constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
 constexpr int kMaxTileStates = 1 << (32 - kEntryPosBits);
-constexpr int kDenseKeyBits = 16;    // prefix tables with keys of <= 16 bits are dense
+constexpr uint64_t kDenseKeys = 1ull << 18;  // prefix tables with <= 2^18 keys are dense
 
 // One prefix-memoization table of depth d for a tile (precompute_table.h:8-101).
-// The key is the class ids of the next d input bytes, kb bits each
-// (kb = TileDev::kb). dense: offsets indexed by the key; otherwise keys[]
-// holds the sorted non-empty keys and offsets are indexed by rank.
+// The key is the class ids c_0 .. c_{d-1} of the next d input bytes as a
+// base-C number (C = TileDev::ncls): ((c_0 * C + c_1) * C + ...) + c_{d-1}.
+// dense: offsets indexed by the key; otherwise keys[] holds the sorted
+// non-empty keys and offsets are indexed by rank.
 struct PrefixTableDev {
   int32_t dense = 0;
   int32_t nkeys = 0;
@@ -49,7 +50,7 @@ struct TileDev {
   int32_t max_path = -1;    // longest path in states if acyclic, else -1
   int32_t ncls = 0;         // byte classes
   int32_t cw = 8;           // class words per state: 1, 2 or 8
-  int32_t kb = 8;           // key bits per class symbol: 5, 6 or 8
+  int32_t pad0 = 0;
   int32_t image_bytes = 0;  // multiple of 16
   int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
   int32_t inj_batch = 32;   // positions injected per worklist refill

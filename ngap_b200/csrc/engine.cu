@@ -150,8 +150,8 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
   ngap_table_opts o{};
   o.precompute_cutoff = -1;
   if (opts) o = *opts;
-  if (o.precompute_depth < 0 || o.precompute_depth > kMaxDepth) {
-    set_error("precompute_depth must be in 0..%d (got %d)", kMaxDepth, o.precompute_depth);
+  if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth) {
+    set_error("precompute_depth must be in -1..%d (got %d)", kMaxDepth, o.precompute_depth);
     return NGAP_E_INVALID;
   }
   std::unique_ptr<ngap_tables> t(new ngap_tables());
@@ -181,7 +181,6 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.max_path = th.max_path;
     d.ncls = th.ncls;
     d.cw = th.cw;
-    d.kb = th.kb;
     d.image_bytes = (int32_t)th.image.size();
     d.off_cmask = th.off_cmask;
     d.off_rep = th.off_rep;

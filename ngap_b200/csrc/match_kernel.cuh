@@ -112,7 +112,8 @@ struct TileView {
   const uint32_t* rep;
   const uint8_t* cls;
   const TileDev* t;
-  int cw, kb;
+  int cw;
+  uint32_t ncls;  // class count: base of the prefix-table keys
   uint32_t gbits;
 };
 
@@ -313,7 +314,7 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
   uint32_t key = 0, vb = 0, ve = 0;
   for (int d = 0; d < depth; d++) {
     const bool act = d < k;
-    if (act) key = (key << tv.kb) | c.in[r + d];
+    if (act) key = key * tv.ncls + c.in[r + d];
     if (t.pt[d].has_reports) {
       uint32_t rb = 0, re = 0;
       if (act) pt_lookup(t.pt[d], key, true, rb, re);
@@ -551,7 +552,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     tv.cls = ib + t->off_cls;
     tv.t = t;
     tv.cw = t->cw;
-    tv.kb = t->kb;
+    tv.ncls = (uint32_t)t->ncls;
     tv.gbits = (uint32_t)t->group << 22;
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? 32 : t->inj_batch;

@@ -99,13 +99,12 @@ inline bool accepts_cls(const TileHost& t, uint32_t v, int c) {
 
 inline bool is_report(const TileHost& t, uint32_t v) { return (t.rep[v >> 5] >> (v & 31)) & 1u; }
 
-void finish_table(PrefixTableHost& pt, int key_bits,
+void finish_table(PrefixTableHost& pt, uint64_t space,
                   const std::map<uint32_t, std::vector<uint32_t>>& lists, const TileHost& t,
                   int cutoff_opt) {
-  pt.dense = key_bits <= kDenseKeyBits;
+  pt.dense = space <= kDenseKeys;
   int64_t total = 0, nonzero = 0;
   if (pt.dense) {
-    const uint64_t space = 1ull << key_bits;
     pt.voff.assign(space + 1, 0);
     pt.roff.assign(space + 1, 0);
     std::vector<uint32_t> vcount(space, 0), rcount(space, 0);
@@ -146,6 +145,7 @@ void finish_table(PrefixTableHost& pt, int key_bits,
       }
     }
   }
+  if (pt.rlist.empty()) pt.roff.assign(1, 0);  // no reports: the offsets are never read
   for (auto& kv : lists) {
     total += (int64_t)kv.second.size();
     nonzero++;
@@ -156,8 +156,10 @@ void finish_table(PrefixTableHost& pt, int key_bits,
 }
 
 void build_prefix_tables(TileHost& t, const TableOpts& opts) {
-  const int want = std::max(1, std::min(opts.precompute_depth, kMaxDepth));
-  const int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)4 << 20;
+  // depth < 0: as deep as the size caps allow
+  const int want = opts.precompute_depth < 0 ? kMaxDepth
+                                             : std::max(1, std::min(opts.precompute_depth, kMaxDepth));
+  const int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)2 << 20;
   std::map<uint32_t, std::vector<uint32_t>> prev, cur;
   for (int c = 0; c < t.ncls; c++) {
     std::vector<uint32_t> l;
@@ -165,11 +167,14 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
       if (accepts_cls(t, a, c)) l.push_back(a);
     if (!l.empty()) prev[(uint32_t)c] = std::move(l);
   }
-  finish_table(t.pt[0], t.kb, prev, t, opts.precompute_cutoff);
+  finish_table(t.pt[0], (uint64_t)t.ncls, prev, t, opts.precompute_cutoff);
+  uint64_t space = (uint64_t)t.ncls;
   t.depth = 1;
   std::vector<uint32_t> mark(t.nstates, 0);
   uint32_t stamp = 0;
   for (int d = 2; d <= want; d++) {
+    if (space * (uint64_t)t.ncls >= (1ull << 32)) break;  // keys are 32-bit
+    space *= (uint64_t)t.ncls;
     cur.clear();
     int64_t total = 0;
     bool too_big = false;
@@ -191,14 +196,14 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
         if (!l.empty()) {
           std::sort(l.begin(), l.end());
           total += (int64_t)l.size();
-          cur[(kv.first << t.kb) | (uint32_t)c] = std::move(l);
+          cur[kv.first * (uint32_t)t.ncls + (uint32_t)c] = std::move(l);
           if (total > cap) too_big = true;
         }
       }
       if (too_big) break;
     }
     if (too_big) break;
-    finish_table(t.pt[d - 1], d * t.kb, cur, t, opts.precompute_cutoff);
+    finish_table(t.pt[d - 1], space, cur, t, opts.precompute_cutoff);
     t.depth = d;
     prev.swap(cur);
   }
@@ -249,11 +254,9 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   t.cls.resize(256);
   if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
     t.ncls = 256;
-    t.kb = 8;
     for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)b;
   } else {
     t.ncls = part.n;
-    t.kb = t.cw == 1 ? 5 : 6;
     for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)part.id[b];
   }
   t.succ.assign((size_t)n * 4, kNoSucc);

@@ -22,7 +22,7 @@ struct TileHost {
   int32_t depth = 0;
   int32_t max_path = -1;
   int32_t num_ccs = 0;
-  int32_t ncls = 0, cw = 8, kb = 8;
+  int32_t ncls = 0, cw = 8;
   int32_t inj_batch = 32;            // positions injected per worklist refill
   std::vector<uint8_t> cls;          // 256: byte -> class
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor

@@ -82,7 +82,24 @@ def test_dotstar_unbounded(engine, algo, window):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("chunk,window,tile_states", [(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
+@pytest.mark.parametrize("depth", [4, 6, -1])
+@pytest.mark.parametrize("gen,kw,g", [
+    (W.hamming_set, dict(seed=17, n_patterns=40, input_len=1 << 17, plant_every=1 << 10), 3),
+    (W.levenshtein_set, dict(seed=18, n_patterns=25, input_len=1 << 16, plant_every=1 << 10), 2),
+    (W.dotstar_set, dict(seed=19, n_patterns=60, input_len=1 << 16, plant_every=1 << 10), 2),
+    (W.literal_set, dict(seed=20, input_len=1 << 16, plant_every=1 << 10), 1),
+])
+def test_deep_prefix_tables(engine, gen, kw, g, depth):
+    """Class-keyed prefix tables deeper than the reference's 3 levels."""
+    anml, data = gen(**kw)
+    for algo in ("nonblockingpcgroups", "nonblockingallgroups"):
+        got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=g, depth=depth,
+                             algorithm=algo)
+        assert len(want) > 0
+        assert np.array_equal(got, want), algo
+
+
+@pytest.mark.parametrize("chunk,window,tile_states",[(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
 def test_chunking_and_tiling(engine, chunk, window, tile_states):
     """Small chunks, windows and tiles exercise warm-up, carry and tile splits."""
     anml, data = W.hamming_set(seed=12, n_patterns=30, input_len=1 << 16, plant_every=1 << 10)
