@@ -3,7 +3,8 @@
 Workload (default): the Hamming k-mer set — 1000 random ACGT 25-mers with <= 3
 substitutions (166k STEs), a 16 MiB ACGT stream with mutated copies every
 64 KiB, cut into 16 segments of 1 MiB (the reference's throughput runs use
-1 MB segments), 10 groups, prefix depth 3, algorithm nonblockingallgroups.
+1 MB segments), 10 groups, prefix memoization as deep as the table caps allow
+(byte-class keys, up to 8 levels), algorithm nonblockingpcgroups.
 A step = one match of the whole stream + device sort/unique of the reports.
 
   value  inputs already in HBM (16 MiB < L2, so L2 is flushed between steps)
@@ -38,15 +39,15 @@ def workload_args(name):
     from ngap_b200 import workloads as W
     if name == "hamming_set":
         anml, data = W.hamming_set(seed=2)
-        return anml, data, dict(group_num=10, depth=3, seg_len=SEG, algorithm="nonblockingallgroups",
+        return anml, data, dict(group_num=10, depth=-1, seg_len=SEG, algorithm="nonblockingpcgroups",
                                 desc="1000 ACGT 25-mers, Hamming <= 3 (166k STEs), 16 MiB, 16 x 1 MiB segments")
     if name == "literal_set":
         anml, data = W.literal_set(seed=1)
-        return anml, data, dict(group_num=1, depth=3, seg_len=len(data), algorithm="nonblockingallgroups",
+        return anml, data, dict(group_num=1, depth=-1, seg_len=len(data), algorithm="nonblockingpcgroups",
                                 desc="64 literals 8-16 B with classes (786 STEs), 1 MiB single segment")
     if name == "high_frontier":
         anml, data = W.high_frontier(seed=3)
-        return anml, data, dict(group_num=10, depth=2, seg_len=SEG, algorithm="nonblockingallgroups",
+        return anml, data, dict(group_num=10, depth=-1, seg_len=SEG, algorithm="nonblockingpcgroups",
                                 desc="500 Levenshtein-2 20-mers + 2000 lit.*lit, 32 MiB, 32 x 1 MiB segments")
     raise SystemExit(f"unknown workload {name}")
 
