@@ -14,33 +14,43 @@ constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
 constexpr int kMaxTileStates = 1 << (32 - kEntryPosBits);
 constexpr uint64_t kDenseKeys = 1ull << 18;  // prefix tables with <= 2^18 keys are dense
 
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+
 // One prefix-memoization table of depth d for a tile (precompute_table.h:8-101).
-// The key is the class ids c_0 .. c_{d-1} of the next d input bytes as a
-// base-C number (C = TileDev::ncls): ((c_0 * C + c_1) * C + ...) + c_{d-1}.
-// dense: offsets indexed by the key; otherwise keys[] holds the sorted
-// non-empty keys and offsets are indexed by rank.
+// The key is the live class ids c_0 .. c_{d-1} of the next d input bytes as a
+// base-L number (L = TileDev::nlive): ((c_0 * L + c_1) * L + ...) + c_{d-1}.
+// A byte of the dead class (accepted by no state of the tile) ends every path,
+// so keys never contain it. dense: offsets indexed by the key (key space
+// <= kDenseKeys); otherwise an open-addressing hash table (linear probing,
+// capacity a power of two, at least twice the keys) whose slots hold
+// {key, state-list begin, report-list begin, state-list length << 16 |
+// report-list length}; the reference binary-searches a sorted key array
+// (precompute_table.h:59-100).
 struct PrefixTableDev {
   int32_t dense = 0;
-  int32_t nkeys = 0;
-  int32_t nrkeys = 0;
+  uint32_t hmask = 0;               // hash capacity - 1
   int32_t cutoff = 0;
   int32_t has_reports = 0;          // any report list non-empty
-  int32_t pad = 0;
-  const uint32_t* keys = nullptr;   // state-list keys (compressed)
-  const uint32_t* voff = nullptr;   // state-list offsets
-  const uint32_t* vlist = nullptr;  // local states reached after d bytes
-  const uint32_t* rkeys = nullptr;  // report-list keys (compressed)
-  const uint32_t* roff = nullptr;   // report-list offsets
-  const uint32_t* rlist = nullptr;  // local report states reached after d bytes
+  const uint32_t* voff = nullptr;   // dense: state-list offsets [space + 1]
+  const uint32_t* roff = nullptr;   // dense: report-list offsets [space + 1] (if reports)
+  const uint4* slots = nullptr;     // hashed: [hmask + 1]
+  const uint32_t* vlist = nullptr;  // local states reached after d symbols
+  const uint32_t* rlist = nullptr;  // local report states reached after d symbols
 };
+
+__host__ __device__ inline uint32_t prefix_hash(uint32_t key) {
+  return (key * 0x9E3779B1u) ^ (key >> 15);
+}
 
 // A tile: a set of whole CCs of one group, matched by one warp per unit.
 // Its hot tables form one contiguous image, staged into shared memory by the
 // CTA that works on the tile:
-//   [succ: nstates x uint4][cmask: nstates x cw x u32][rep: ceil(nstates/32) x u32][cls: 256 B]
-// succ: up to 4 tile-local successors, bit 31 = successor is a report state,
-// kNoSucc = none. cmask: bit c of word c/32 = the state accepts byte class c.
-// cls: byte -> class (identity when cw == 8).
+//   [succ][cmask: nstates x cw x u32][rep: ceil(nstates/32) x u32][cls: 256 B]
+// succ: up to 4 tile-local successors per state; narrow tiles (< 32767
+// states) store 4 x u16 (bit 15 = report successor, 0xffff = none), wide
+// ones 4 x u32 (bit 31 = report successor, kNoSucc = none). cmask: bit c of
+// word c/32 = the state accepts byte class c. cls: byte -> class id, live
+// classes first (identity when cw == 8).
 struct TileDev {
   int32_t group = 0;
   int32_t nstates = 0;
@@ -50,7 +60,8 @@ struct TileDev {
   int32_t max_path = -1;    // longest path in states if acyclic, else -1
   int32_t ncls = 0;         // byte classes
   int32_t cw = 8;           // class words per state: 1, 2 or 8
-  int32_t pad0 = 0;
+  int32_t nlive = 0;        // live classes: key base; class id nlive = dead
+  int32_t narrow = 1;       // 16-bit successors
   int32_t image_bytes = 0;  // multiple of 16
   int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
   int32_t inj_batch = 32;   // positions injected per worklist refill

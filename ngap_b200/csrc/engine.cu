@@ -181,6 +181,8 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.max_path = th.max_path;
     d.ncls = th.ncls;
     d.cw = th.cw;
+    d.nlive = th.nlive;
+    d.narrow = th.narrow ? 1 : 0;
     d.image_bytes = (int32_t)th.image.size();
     d.off_cmask = th.off_cmask;
     d.off_rep = th.off_rep;
@@ -194,15 +196,15 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       const PrefixTableHost& ph = th.pt[k];
       PrefixTableDev& pd = d.pt[k];
       pd.dense = ph.dense ? 1 : 0;
-      pd.nkeys = (int32_t)ph.keys.size();
-      pd.nrkeys = (int32_t)ph.rkeys.size();
+      pd.hmask = ph.hmask;
       pd.cutoff = ph.cutoff;
       pd.has_reports = ph.rlist.empty() ? 0 : 1;
-      if ((rc = t->upload(ph.keys, &pd.keys)) != NGAP_OK) return rc;
       if ((rc = t->upload(ph.voff, &pd.voff)) != NGAP_OK) return rc;
-      if ((rc = t->upload(ph.vlist, &pd.vlist)) != NGAP_OK) return rc;
-      if ((rc = t->upload(ph.rkeys, &pd.rkeys)) != NGAP_OK) return rc;
       if ((rc = t->upload(ph.roff, &pd.roff)) != NGAP_OK) return rc;
+      const uint32_t* slots = nullptr;
+      if ((rc = t->upload(ph.slots, &slots)) != NGAP_OK) return rc;
+      pd.slots = reinterpret_cast<const uint4*>(slots);
+      if ((rc = t->upload(ph.vlist, &pd.vlist)) != NGAP_OK) return rc;
       if ((rc = t->upload(ph.rlist, &pd.rlist)) != NGAP_OK) return rc;
     }
     t->dev_desc.push_back(d);
@@ -489,6 +491,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   int rc = ensure_reports(e, cap);
   if (rc != NGAP_OK) return rc;
   // shared memory: the largest tile image that fits the budget, plus the warps
+  // (a window too large for what is left is shortened)
+  while (window > 64 && cta_smem_bytes(window, t->image_region) > 227 * 1024 - 1024) window /= 2;
   const int smem = cta_smem_bytes(window, t->image_region);
   if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
   int bps = 0;

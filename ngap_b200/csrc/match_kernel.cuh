@@ -38,7 +38,7 @@ namespace ngap {
 
 constexpr int kWarpsPerCta = 16;
 constexpr int kCtaThreads = kWarpsPerCta * 32;
-constexpr int kStackCap = 1024;   // entries per warp in shared memory
+constexpr int kStackCap = 512;    // entries per warp in shared memory
 constexpr int kReportBuf = 64;    // reports per warp buffered in shared memory
 constexpr int kInjectLow = 256;   // inject new positions while the stack holds fewer entries
 constexpr unsigned kFull = 0xffffffffu;
@@ -107,15 +107,28 @@ struct WarpRun {
 // The tile a warp works on: hot tables in shared memory (or global memory
 // when the image does not fit) and the cold ones in global memory.
 struct TileView {
-  const uint4* succ;
+  const uint4* succ;    // wide tiles
+  const uint2* succ2;   // narrow tiles: 4 x u16
   const uint32_t* cmask;
   const uint32_t* rep;
   const uint8_t* cls;
   const TileDev* t;
+  const PrefixTableDev* pt;  // the tile's prefix tables (shared-memory copy)
   int cw;
-  uint32_t ncls;  // class count: base of the prefix-table keys
+  int narrow;
+  uint32_t nlive;  // live classes: base of the prefix-table keys
   uint32_t gbits;
 };
+
+// Successors of v in the 32-bit convention (bit 31 = report, kNoSucc = none).
+__device__ __forceinline__ uint4 load_succ(const TileView& tv, uint32_t v) {
+  if (!tv.narrow) return tv.succ[v];
+  const uint2 x = tv.succ2[v];
+  auto wide = [](uint32_t h) {
+    return h == 0xffffu ? kNoSucc : ((h & 0x7fffu) | ((h & 0x8000u) << 16));
+  };
+  return make_uint4(wide(x.x & 0xffffu), wide(x.x >> 16), wide(x.y & 0xffffu), wide(x.y >> 16));
+}
 
 // Everything about the current unit and window.
 struct UnitCtx {
@@ -264,28 +277,36 @@ __device__ __forceinline__ void carry_state(const MatchParams& p, WarpRun& w, in
   __syncwarp();
 }
 
-// Looks up key in a prefix table; returns [b, e) of its state (or report) list.
-__device__ __forceinline__ void pt_lookup(const PrefixTableDev& t, uint32_t key, bool reports,
-                                          uint32_t& b, uint32_t& e) {
-  const uint32_t* off = reports ? t.roff : t.voff;
+// Looks up key in a prefix table: [vb, ve) of its state list when want_v and
+// [rb, re) of its report list when want_r; empty ranges when absent.
+__device__ __forceinline__ void pt_find(const PrefixTableDev& t, uint32_t key, bool want_v,
+                                        bool want_r, uint32_t& vb, uint32_t& ve, uint32_t& rb,
+                                        uint32_t& re) {
+  vb = ve = rb = re = 0;
+  if (!want_v && !want_r) return;
   if (t.dense) {
-    b = __ldg(off + key);
-    e = __ldg(off + key + 1);
+    if (want_v) {
+      vb = __ldg(t.voff + key);
+      ve = __ldg(t.voff + key + 1);
+    }
+    if (want_r) {
+      rb = __ldg(t.roff + key);
+      re = __ldg(t.roff + key + 1);
+    }
     return;
   }
-  const uint32_t* keys = reports ? t.rkeys : t.keys;
-  int lo = 0, hi = (reports ? t.nrkeys : t.nkeys) - 1;
-  b = e = 0;
-  while (lo <= hi) {
-    const int mid = (lo + hi) >> 1;
-    const uint32_t k = __ldg(keys + mid);
-    if (k == key) {
-      b = __ldg(off + mid);
-      e = __ldg(off + mid + 1);
+  uint32_t h = prefix_hash(key) & t.hmask;
+  for (uint32_t probe = 0; probe <= t.hmask; probe++) {  // at least half the slots are empty
+    const uint4 s = __ldg(t.slots + h);
+    if (s.x == key) {
+      vb = s.y;
+      ve = s.y + (s.w >> 16);
+      rb = s.z;
+      re = s.z + (s.w & 0xffffu);
       return;
     }
-    if (k < key) lo = mid + 1;
-    else hi = mid - 1;
+    if (s.x == kHashEmpty) return;
+    h = (h + 1) & t.hmask;
   }
 }
 
@@ -309,27 +330,39 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
     }
     return;
   }
-  // table depth clamped at the window end: states land at q + k - 1 < window end
-  const int k = valid ? min(depth, c.wlen - r) : 0;
+  // table depth clamped at the window end: states land at q + k - 1 < window end;
+  // a dead-class symbol at offset d ends every path, so only reports of the
+  // first d symbols remain and no state needs expanding
+  const int kmax = valid ? min(depth, c.wlen - r) : 0;
+  int k = kmax;
+  for (int d = 0; d < depth; d++)
+    if (d < k && c.in[r + d] >= tv.nlive) k = d;
+  const bool keep_states = k == kmax;
   uint32_t key = 0, vb = 0, ve = 0;
   for (int d = 0; d < depth; d++) {
     const bool act = d < k;
-    if (act) key = key * tv.ncls + c.in[r + d];
-    if (t.pt[d].has_reports) {
-      uint32_t rb = 0, re = 0;
-      if (act) pt_lookup(t.pt[d], key, true, rb, re);
+    if (act) key = key * tv.nlive + c.in[r + d];
+    const PrefixTableDev& pt = tv.pt[d];
+    const bool want_v = act && keep_states && d == k - 1;
+    const bool want_r = act && pt.has_reports;
+    uint32_t b0, e0, rb, re;
+    pt_find(pt, key, want_v, want_r, b0, e0, rb, re);
+    if (want_v) {
+      vb = b0;
+      ve = e0;
+    }
+    if (pt.has_reports) {
       const int len = (int)(re - rb);
       const int mx = __reduce_max_sync(kFull, len);
       for (int i = 0; i < mx; i++) {
         const bool ok = i < len && q + d >= c.emit_lo;
-        const uint32_t v = ok ? __ldg(t.pt[d].rlist + rb + i) : 0u;
+        const uint32_t v = ok ? __ldg(pt.rlist + rb + i) : 0u;
         emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v) | tv.gbits) : 0u, (uint32_t)(q + d));
       }
     }
-    if (act && d == k - 1) pt_lookup(t.pt[d], key, false, vb, ve);
   }
   // entries at the unit's last position have nothing to expand
-  const uint32_t len = (k > 0 && q + k < c.hi) ? (ve - vb) : 0u;
+  const uint32_t len = (keep_states && k > 0 && q + k < c.hi) ? (ve - vb) : 0u;
   n_injected += len;
   uint32_t incl = len;
 #pragma unroll
@@ -353,7 +386,7 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
     }
     const uint32_t before = l0 > 0 ? ws.inj[l0 - 1] : 0u;
     const int kk = (int)ws.inj[64 + l0];
-    const uint32_t v = __ldg(t.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
+    const uint32_t v = __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
     store_entry(p, ws, w, w.top + (int)idx, (v << kEntryPosBits) | (uint32_t)(r0 + l0 + kk - 1));
   }
   grow_stack(p, w, (int)total);
@@ -397,7 +430,7 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
   uint4 sc = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
   uint32_t s = 0;
   if (go) {
-    sc = tv.succ[v];
+    sc = load_succ(tv, v);
     s = c.in[r + 1];
   }
   n_expanded += go;
@@ -443,7 +476,7 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     uint4 sc2 = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
-    if (inner && ok[j]) sc2 = tv.succ[u[j] & kIdMask];
+    if (inner && ok[j]) sc2 = load_succ(tv, u[j] & kIdMask);
     u2[j][0] = sc2.x;
     u2[j][1] = sc2.y;
     u2[j][2] = sc2.z;
@@ -486,6 +519,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   __shared__ int s_task;
   __shared__ unsigned s_next;
+  __shared__ __align__(16) PrefixTableDev s_pt[kMaxDepth];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = p.window;
   uint8_t* image = smem_raw;
@@ -542,17 +576,25 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       for (int i = threadIdx.x; i < t->image_bytes / 16; i += kCtaThreads) dst[i] = __ldg(src + i);
       staged = tk.tile;
     }
+    {  // the tile's prefix-table descriptors, read at every injection
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(t->pt);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(s_pt);
+      for (int i = threadIdx.x; i < (int)(sizeof(s_pt) / 4); i += kCtaThreads) dst[i] = src[i];
+    }
     if (threadIdx.x == 0) s_next = (unsigned)tk.ubegin;
     __syncthreads();
     TileView tv;
     const uint8_t* ib = fits ? image : t->image;
     tv.succ = reinterpret_cast<const uint4*>(ib);
+    tv.succ2 = reinterpret_cast<const uint2*>(ib);
     tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
     tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
     tv.cls = ib + t->off_cls;
     tv.t = t;
+    tv.pt = s_pt;
     tv.cw = t->cw;
-    tv.ncls = (uint32_t)t->ncls;
+    tv.narrow = t->narrow;
+    tv.nlive = (uint32_t)t->nlive;
     tv.gbits = (uint32_t)t->group << 22;
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? 32 : t->inj_batch;

@@ -99,9 +99,11 @@ inline bool accepts_cls(const TileHost& t, uint32_t v, int c) {
 
 inline bool is_report(const TileHost& t, uint32_t v) { return (t.rep[v >> 5] >> (v & 31)) & 1u; }
 
-void finish_table(PrefixTableHost& pt, uint64_t space,
+// Lays out one table; false when a list is too long for the hashed slot format.
+bool finish_table(PrefixTableHost& pt, uint64_t space,
                   const std::map<uint32_t, std::vector<uint32_t>>& lists, const TileHost& t,
                   int cutoff_opt) {
+  pt = PrefixTableHost();
   pt.dense = space <= kDenseKeys;
   int64_t total = 0, nonzero = 0;
   if (pt.dense) {
@@ -127,25 +129,29 @@ void finish_table(PrefixTableHost& pt, uint64_t space,
       }
     }
   } else {
-    pt.voff.push_back(0);
-    pt.roff.push_back(0);
+    uint64_t cap = 16;
+    while (cap < 2 * lists.size()) cap <<= 1;
+    pt.hmask = (uint32_t)(cap - 1);
+    pt.slots.assign(cap * 4, 0);
+    for (uint64_t s = 0; s < cap; s++) pt.slots[s * 4] = kHashEmpty;
     for (auto& kv : lists) {
-      pt.keys.push_back(kv.first);
-      for (uint32_t v : kv.second) pt.vlist.push_back(v);
-      pt.voff.push_back((uint32_t)pt.vlist.size());
-      bool any = false;
-      for (uint32_t v : kv.second)
-        if (is_report(t, v)) {
-          pt.rlist.push_back(v);
-          any = true;
-        }
-      if (any) {
-        pt.rkeys.push_back(kv.first);
-        pt.roff.push_back((uint32_t)pt.rlist.size());
+      const uint32_t vb = (uint32_t)pt.vlist.size(), rb = (uint32_t)pt.rlist.size();
+      for (uint32_t v : kv.second) {
+        pt.vlist.push_back(v);
+        if (is_report(t, v)) pt.rlist.push_back(v);
       }
+      const uint32_t vl = (uint32_t)pt.vlist.size() - vb, rl = (uint32_t)pt.rlist.size() - rb;
+      if (vl >= 65536 || rl >= 65536) return false;
+      uint32_t h = prefix_hash(kv.first) & pt.hmask;
+      while (pt.slots[(size_t)h * 4] != kHashEmpty) h = (h + 1) & pt.hmask;
+      uint32_t* sl = &pt.slots[(size_t)h * 4];
+      sl[0] = kv.first;
+      sl[1] = vb;
+      sl[2] = rb;
+      sl[3] = (vl << 16) | rl;
     }
   }
-  if (pt.rlist.empty()) pt.roff.assign(1, 0);  // no reports: the offsets are never read
+  if (pt.rlist.empty()) pt.roff.clear();  // no reports: the offsets are never read
   for (auto& kv : lists) {
     total += (int64_t)kv.second.size();
     nonzero++;
@@ -153,6 +159,7 @@ void finish_table(PrefixTableHost& pt, uint64_t space,
   // PrecTable::calcCutoff (precompute_table.cu:171-186): mean non-empty list length.
   pt.cutoff = nonzero > 0 ? (int32_t)(total / nonzero) : 0;
   if (cutoff_opt >= 0) pt.cutoff = cutoff_opt;
+  return true;
 }
 
 void build_prefix_tables(TileHost& t, const TableOpts& opts) {
@@ -160,26 +167,28 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
   const int want = opts.precompute_depth < 0 ? kMaxDepth
                                              : std::max(1, std::min(opts.precompute_depth, kMaxDepth));
   const int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)2 << 20;
+  // keys are base-L numbers over the L live classes (the dead class ends paths)
+  const uint32_t L = (uint32_t)t.nlive;
   std::map<uint32_t, std::vector<uint32_t>> prev, cur;
-  for (int c = 0; c < t.ncls; c++) {
+  for (uint32_t c = 0; c < L; c++) {
     std::vector<uint32_t> l;
     for (uint32_t a : t.aas)
-      if (accepts_cls(t, a, c)) l.push_back(a);
-    if (!l.empty()) prev[(uint32_t)c] = std::move(l);
+      if (accepts_cls(t, a, (int)c)) l.push_back(a);
+    if (!l.empty()) prev[c] = std::move(l);
   }
-  finish_table(t.pt[0], (uint64_t)t.ncls, prev, t, opts.precompute_cutoff);
-  uint64_t space = (uint64_t)t.ncls;
+  finish_table(t.pt[0], (uint64_t)L, prev, t, opts.precompute_cutoff);
+  uint64_t space = (uint64_t)L;
   t.depth = 1;
   std::vector<uint32_t> mark(t.nstates, 0);
   uint32_t stamp = 0;
   for (int d = 2; d <= want; d++) {
-    if (space * (uint64_t)t.ncls >= (1ull << 32)) break;  // keys are 32-bit
-    space *= (uint64_t)t.ncls;
+    if (space * (uint64_t)L >= (1ull << 32)) break;  // keys are 32-bit
+    space *= (uint64_t)L;
     cur.clear();
     int64_t total = 0;
     bool too_big = false;
     for (auto& kv : prev) {
-      for (int c = 0; c < t.ncls && !too_big; c++) {
+      for (int c = 0; c < (int)L && !too_big; c++) {
         std::vector<uint32_t> l;
         stamp++;
         for (uint32_t v : kv.second) {
@@ -196,14 +205,17 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
         if (!l.empty()) {
           std::sort(l.begin(), l.end());
           total += (int64_t)l.size();
-          cur[kv.first * (uint32_t)t.ncls + (uint32_t)c] = std::move(l);
+          cur[kv.first * L + (uint32_t)c] = std::move(l);
           if (total > cap) too_big = true;
         }
       }
       if (too_big) break;
     }
     if (too_big) break;
-    finish_table(t.pt[d - 1], space, cur, t, opts.precompute_cutoff);
+    if (!finish_table(t.pt[d - 1], space, cur, t, opts.precompute_cutoff)) {
+      t.pt[d - 1] = PrefixTableHost();
+      break;
+    }
     t.depth = d;
     prev.swap(cur);
   }
@@ -217,11 +229,21 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
 void build_image(TileHost& t) {
   auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
   const size_t n = (size_t)t.nstates;
-  t.off_cmask = (int32_t)r16(n * 16);
+  t.narrow = t.nstates <= kNarrowMaxStates;
+  t.off_cmask = (int32_t)r16(n * (t.narrow ? 8 : 16));
   t.off_rep = t.off_cmask + (int32_t)r16(n * t.cw * 4);
   t.off_cls = t.off_rep + (int32_t)r16(((n + 31) / 32) * 4);
   t.image.assign((size_t)t.off_cls + 256, 0);
-  memcpy(t.image.data(), t.succ.data(), n * 16);
+  if (t.narrow) {  // 4 x u16 per state: 15-bit id, bit 15 = report, 0xffff = none
+    uint16_t* s16 = reinterpret_cast<uint16_t*>(t.image.data());
+    for (size_t i = 0; i < n * 4; i++) {
+      const uint32_t u = t.succ[i];
+      s16[i] = u == kNoSucc ? (uint16_t)0xffff
+                            : (uint16_t)((u & 0x7fffu) | ((u >> 31) ? 0x8000u : 0u));
+    }
+  } else {
+    memcpy(t.image.data(), t.succ.data(), n * 16);
+  }
   memcpy(t.image.data() + t.off_cmask, t.cmask.data(), n * t.cw * 4);
   memcpy(t.image.data() + t.off_rep, t.rep.data(), t.rep.size() * 4);
   memcpy(t.image.data() + t.off_cls, t.cls.data(), 256);
@@ -254,10 +276,24 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   t.cls.resize(256);
   if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
     t.ncls = 256;
+    t.nlive = 256;
     for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)b;
   } else {
+    // bytes no state accepts share one (dead) class; number it last
+    uint32_t any[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (auto& c : ccs)
+      for (int32_t v = c.begin; v < c.end; v++)
+        for (int w = 0; w < 8; w++) any[w] |= g.bits[(size_t)v * 8 + w];
+    int dead = -1;
+    for (int b = 0; b < 256 && dead < 0; b++)
+      if (!((any[b >> 5] >> (b & 31)) & 1u)) dead = part.id[b];
     t.ncls = part.n;
-    for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)part.id[b];
+    t.nlive = dead < 0 ? part.n : part.n - 1;
+    for (int b = 0; b < 256; b++) {
+      int id = part.id[b];
+      if (dead >= 0) id = id == dead ? part.n - 1 : (id > dead ? id - 1 : id);
+      t.cls[b] = (uint8_t)id;
+    }
   }
   t.succ.assign((size_t)n * 4, kNoSucc);
   t.bits.resize((size_t)n * 8);

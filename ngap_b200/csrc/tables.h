@@ -12,8 +12,10 @@ namespace ngap {
 struct PrefixTableHost {
   bool dense = false;
   int32_t cutoff = 0;
-  std::vector<uint32_t> keys, voff, vlist;
-  std::vector<uint32_t> rkeys, roff, rlist;
+  uint32_t hmask = 0;
+  std::vector<uint32_t> voff, roff;   // dense
+  std::vector<uint32_t> slots;        // hashed: 4 words per slot
+  std::vector<uint32_t> vlist, rlist;
 };
 
 struct TileHost {
@@ -22,9 +24,10 @@ struct TileHost {
   int32_t depth = 0;
   int32_t max_path = -1;
   int32_t num_ccs = 0;
-  int32_t ncls = 0, cw = 8;
+  int32_t ncls = 0, cw = 8, nlive = 0;
+  bool narrow = true;                // 16-bit successor ids in the image
   int32_t inj_batch = 32;            // positions injected per worklist refill
-  std::vector<uint8_t> cls;          // 256: byte -> class
+  std::vector<uint8_t> cls;          // 256: byte -> class, live classes first
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
   std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
   std::vector<uint32_t> cmask;       // nstates * cw
@@ -41,14 +44,17 @@ struct TableOpts {
   int precompute_cutoff = -1;
   int tile_states = 0;              // max states per tile; 0 = fill the image budget
   int64_t max_table_entries = 0;    // 0 = automatic
-  int image_budget = 96 * 1024;     // bytes of shared memory for one tile's image
+  int image_budget = 144 * 1024;    // bytes of shared memory for one tile's image
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
 };
+
+constexpr int32_t kNarrowMaxStates = 32767;  // 15-bit tile-local ids
 
 // Bytes of a tile image with n states and cw class words.
 inline int64_t image_bytes(int64_t n, int cw) {
   auto r16 = [](int64_t x) { return (x + 15) & ~(int64_t)15; };
-  return r16(n * 16) + r16(n * cw * 4) + r16(((n + 31) / 32) * 4) + 256;
+  const int64_t succ = n <= kNarrowMaxStates ? n * 8 : n * 16;
+  return r16(succ) + r16(n * cw * 4) + r16(((n + 31) / 32) * 4) + 256;
 }
 
 // Splits every group into tiles and builds each tile's tables.
