@@ -4,7 +4,7 @@ Workload (default): the Hamming k-mer set — 1000 random ACGT 25-mers with <= 3
 substitutions (166k STEs), a 16 MiB ACGT stream with mutated copies every
 64 KiB, cut into 16 segments of 1 MiB (the reference's throughput runs use
 1 MB segments), 10 groups, prefix memoization as deep as the table caps allow
-(byte-class keys, up to 8 levels), algorithm nonblockingpcgroups.
+(byte-class keys, up to 12 levels), algorithm nonblockingpcgroups.
 A step = one match of the whole stream + device sort/unique of the reports.
 
   value  inputs already in HBM (16 MiB < L2, so L2 is flushed between steps)

@@ -99,7 +99,7 @@ void ngap_groups_destroy(ngap_groups* g);
 
 typedef struct ngap_table_opts {
   int device;            /* CUDA device ordinal */
-  int precompute_depth;  /* --precompute-depth: prefix-memoization depth 0..8 (the
+  int precompute_depth;  /* --precompute-depth: prefix-memoization depth 0..12 (the
                             reference allows 0..3; keys are byte-class ids, so
                             deeper tables stay small); -1 = as deep as the size
                             caps allow */

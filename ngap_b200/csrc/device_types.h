@@ -8,7 +8,7 @@
 namespace ngap {
 
 constexpr uint32_t kNoSucc = 0xffffffffu;
-constexpr int kMaxDepth = 8;         // prefix-memoization depth limit (the reference stops at 3)
+constexpr int kMaxDepth = 12;        // prefix-memoization depth limit (the reference stops at 3)
 constexpr int kEntryPosBits = 13;    // worklist entry = local_state << 13 | window offset
 constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
 constexpr int kMaxTileStates = 1 << (32 - kEntryPosBits);

@@ -216,6 +216,18 @@ void build_prefix_tables(TileHost& t, const TableOpts& opts) {
       t.pt[d - 1] = PrefixTableHost();
       break;
     }
+    if (opts.precompute_depth < 0) {  // automatic depth: bounded device bytes per tile
+      int64_t bytes = 0;
+      for (int k = 0; k < d; k++) {
+        const PrefixTableHost& pk = t.pt[k];
+        bytes += 4 * (int64_t)(pk.voff.size() + pk.roff.size() + pk.slots.size() +
+                               pk.vlist.size() + pk.rlist.size());
+      }
+      if (bytes > opts.auto_table_bytes) {
+        t.pt[d - 1] = PrefixTableHost();
+        break;
+      }
+    }
     t.depth = d;
     prev.swap(cur);
   }
@@ -344,7 +356,12 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
 
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles) {
   tiles.clear();
-  const int64_t max_states = opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2;
+  // Acyclic tiles get parallelism from chunks, so they fill the image budget.
+  // A cyclic tile is one sequential unit per segment, so those stay small to
+  // give the GPU enough independent units.
+  const int64_t max_states[2] = {
+      opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2,
+      opts.tile_states > 0 ? opts.tile_states : (int64_t)opts.unbounded_tile_states};
   for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
     const GroupGraph& g = gs.groups[gi];
     std::vector<CcInfo> open[2];  // [0] bounded, [1] unbounded
@@ -362,7 +379,7 @@ int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>
       const int32_t sz = ci.end - ci.begin;
       Partition trial = open_part[k];
       for (int32_t v = ci.begin; v < ci.end; v++) trial.refine(&g.bits[(size_t)v * 8]);
-      const bool fits = open_n[k] + sz <= max_states &&
+      const bool fits = open_n[k] + sz <= max_states[k] &&
                         image_bytes(open_n[k] + sz, class_words(trial.n)) <= opts.image_budget;
       if (!open[k].empty() && !fits) {
         if (!emit_tile(g, gi, open[k], opts, tiles)) return degree_error();

@@ -45,6 +45,8 @@ struct TableOpts {
   int tile_states = 0;              // max states per tile; 0 = fill the image budget
   int64_t max_table_entries = 0;    // 0 = automatic
   int image_budget = 144 * 1024;    // bytes of shared memory for one tile's image
+  int unbounded_tile_states = 256;  // cap for tiles of cyclic CCs (one unit per segment)
+  int64_t auto_table_bytes = 12 << 20;  // automatic depth: prefix-table bytes per tile
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
 };
 
