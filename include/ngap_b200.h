@@ -161,6 +161,47 @@ int ngap_last_launches(const ngap_engine* e);
 /* Worklist entries expanded and always-active entries injected by the last match. */
 int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injected);
 
+/* ---- batched matching: many streams, several NFAs, one launch ---- */
+
+/* The reference matches one (duplicated) stream against one NFA per run
+ * (code/src/ngap/main.cu:81-131) with a rigid (group, segment) grid
+ * (code/src/ngap/ngap.cu:1507). A tableset combines the tables of several
+ * NFAs so that streams of uneven length, each against its own NFA, run in one
+ * persistent launch. The tables must outlive the tableset. */
+typedef struct ngap_tableset ngap_tableset;
+int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset** out);
+void ngap_tableset_destroy(ngap_tableset* ts);
+
+typedef struct ngap_batch_stream {
+  uint64_t offset;  /* first byte of the stream in the batch input */
+  uint64_t length;  /* bytes; the stream is one segment (start-of-data states at its start) */
+  int32_t nfa;      /* index into the tableset */
+  int32_t pad;
+} ngap_batch_stream;
+
+typedef struct ngap_batch_params {
+  int algorithm;            /* NGAP_ALGO_* */
+  int unique;
+  int active_threshold;
+  int report_off;
+  uint64_t result_capacity;
+  int window;               /* 0 = automatic */
+  int chunk;                /* 0 = automatic */
+  int use_graph;            /* capture the pipeline in a CUDA graph; replay it while the
+                               tableset, streams, parameters and input pointer repeat */
+} ngap_batch_params;
+
+/* Matches every stream against its NFA in one persistent launch, then sorts
+ * the reports by (stream, offset, id) on the device. Asynchronous on stream;
+ * ngap_engine_sync waits. Offsets in the results are local to each stream. */
+int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* input,
+                     uint64_t input_bytes, int input_on_device, const ngap_batch_stream* streams,
+                     int nstreams, const ngap_batch_params* p, void* stream);
+/* Copies up to cap unique reports (reference encoding) and, when stream_ids is
+ * not NULL, the stream index of each; *n receives the count copied. */
+int ngap_batch_results(ngap_engine* e, uint64_t* reports, uint32_t* stream_ids, uint64_t cap,
+                       uint64_t* n);
+
 /* ---- report compaction ---- */
 
 /* Sorts n packed reports (reference encoding) in device memory by (offset, id)

@@ -5,7 +5,9 @@ for sm_100a in ngap_b200/csrc.
 """
 from ._lib import ALGORITHMS, LIB_PATH, NgapError, lib  # noqa: F401
 from .engine import (Engine, GroupGraph, Groups, Ngap, NgapOption, Nfa, Tables,  # noqa: F401
-                     cpu_validate, decode_reports)
+                     TableSet, batch_match_async, batch_results, cpu_validate, decode_reports,
+                     split_by_stream)
 
 __all__ = ["ALGORITHMS", "Engine", "GroupGraph", "Groups", "Ngap", "NgapOption", "Nfa", "Tables",
-           "NgapError", "cpu_validate", "decode_reports", "lib", "LIB_PATH"]
+           "TableSet", "NgapError", "batch_match_async", "batch_results", "cpu_validate",
+           "decode_reports", "lib", "LIB_PATH", "split_by_stream"]

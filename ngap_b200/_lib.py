@@ -62,6 +62,18 @@ class MatchParams(ctypes.Structure):
                 ("chunk", ctypes.c_int), ("first_segment", ctypes.c_int64)]
 
 
+class BatchStream(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_uint64), ("length", ctypes.c_uint64),
+                ("nfa", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class BatchParams(ctypes.Structure):
+    _fields_ = [("algorithm", ctypes.c_int), ("unique", ctypes.c_int),
+                ("active_threshold", ctypes.c_int), ("report_off", ctypes.c_int),
+                ("result_capacity", ctypes.c_uint64), ("window", ctypes.c_int),
+                ("chunk", ctypes.c_int), ("use_graph", ctypes.c_int)]
+
+
 # name -> (restype, argtypes); exactly the functions include/ngap_b200.h declares
 SIGNATURES = {
     "ngap_nfa_load_anml": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
@@ -97,6 +109,15 @@ SIGNATURES = {
     "ngap_last_launches": (ctypes.c_int, [ctypes.c_void_p]),
     "ngap_engine_work": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "ngap_tableset_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "ngap_tableset_destroy": (None, [ctypes.c_void_p]),
+    "ngap_batch_match": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_uint64, ctypes.c_int,
+                                        ctypes.POINTER(BatchStream), ctypes.c_int,
+                                        ctypes.POINTER(BatchParams), ctypes.c_void_p]),
+    "ngap_batch_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "ngap_reports_sort_unique": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                                 ctypes.c_void_p]),

@@ -73,11 +73,15 @@ struct TileDev {
 };
 
 // A unit of work: one tile over input positions [lo, hi); reports are kept for
-// positions >= emit_lo (the positions before are warm-up of a chunk).
+// positions >= emit_lo (the positions before are warm-up of a chunk). A report
+// at position q is stored as key_hi | (q - base) << off_shift | id, where
+// key_hi carries the stream index in batched matching (0 otherwise).
 struct UnitDev {
   int32_t tile;
   uint32_t flags;  // bit0: inject start-of-data states at lo
   int64_t lo, hi, emit_lo;
+  int64_t base;      // first byte of the unit's stream
+  uint64_t key_hi;   // stream index, already shifted into the report key
 };
 
 // A CTA-level task: consecutive units [ubegin, uend) of one tile.

@@ -118,6 +118,18 @@ struct ngap_engine {
   int pending_status = NGAP_OK;
   bool ran = false;
   int grid = 0;
+  // batched matching
+  const void* batch_ts = nullptr;
+  std::vector<ngap_batch_stream> batch_streams;
+  int batch_window = -1, batch_chunk = -1;
+  uint32_t* d_stream_ids = nullptr;
+  uint64_t stream_ids_cap = 0;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<uint64_t> graph_key;
+  bool graph_mode = false;
+  int graph_launches = 0;
+  cudaStream_t cap_stream = nullptr;  // capture/replay stream of the batched graph
+  cudaEvent_t cap_ev[2] = {nullptr, nullptr};
 
   ~ngap_engine() {
     cudaFree(d_input);
@@ -133,6 +145,11 @@ struct ngap_engine {
     cudaFree(d_carry);
     cudaFree(d_marks);
     cudaFree(d_ovf);
+    cudaFree(d_stream_ids);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& c : cap_ev)
+      if (c) cudaEventDestroy(c);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
     if (h_counters) cudaFreeHost(h_counters);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
@@ -305,43 +322,52 @@ int ensure_slots(ngap_engine* e, size_t slots, int max_states) {
 // one tile are then cut into CTA tasks: the long per-segment units of
 // unbounded tiles one per warp of a task and first, the chunks after them in
 // tasks sized to give every CTA several tasks.
-void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vector<UnitDev>& units,
-                std::vector<TaskDev>& tasks) {
+// One independent input range (a segment, or a whole stream in batched mode).
+struct SegSpec {
+  int64_t lo, hi;
+  bool starts;      // start-of-data states active at lo
+  uint64_t key_hi;  // stream index in the report key
+  int64_t base;     // offsets in reports are relative to this
+};
+
+void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int chunk_opt,
+               std::vector<UnitDev>& unbounded, std::vector<UnitDev>& bounded) {
+  UnitDev u{};
+  u.tile = tile;
+  u.key_hi = s.key_hi;
+  u.base = s.base;
+  const bool starts = s.starts && !th.start.empty();
+  if (th.max_path < 0) {
+    u.flags = starts ? 1u : 0u;
+    u.lo = s.lo;
+    u.hi = s.hi;
+    u.emit_lo = s.lo;
+    unbounded.push_back(u);
+    return;
+  }
+  const int64_t warm = th.max_path > 0 ? th.max_path - 1 : 0;
+  // chunk length is independent of the window (the blocking algorithm runs
+  // one-position windows); a chunk should span at least its warm-up
+  const int64_t base = std::max<int64_t>(window, 2048);
+  int64_t chunk = chunk_opt > 0 ? chunk_opt : std::max<int64_t>(base - warm, base / 2);
+  chunk = std::max<int64_t>(chunk, 1);
+  for (int64_t em = s.lo; em < s.hi; em += chunk) {
+    u.lo = std::max(s.lo, em - warm);
+    u.hi = std::min(em + chunk, s.hi);
+    u.emit_lo = em;
+    u.flags = (starts && u.lo == s.lo) ? 1u : 0u;
+    bounded.push_back(u);
+  }
+}
+
+// Units (already grouped by tile) -> CTA tasks: the long units of cyclic tiles
+// first, one per warp of a task; chunks after them in tasks sized to give
+// every CTA several tasks.
+void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& unbounded,
+                const std::vector<UnitDev>& bounded, int grid, std::vector<TaskDev>& tasks) {
   units.clear();
   tasks.clear();
-  std::vector<UnitDev> bounded;
-  for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
-    const TileHost& th = t->tiles[ti];
-    for (int64_t s = 0; s < k.num_seg; s++) {
-      const int64_t slo = s * k.seg_len, shi = slo + k.seg_len;
-      const bool starts = (k.first_seg + s == 0 || k.is_dup) && !th.start.empty();
-      if (th.max_path < 0) {
-        UnitDev u;
-        u.tile = ti;
-        u.flags = starts ? 1u : 0u;
-        u.lo = slo;
-        u.hi = shi;
-        u.emit_lo = slo;
-        units.push_back(u);
-        continue;
-      }
-      const int64_t warm = th.max_path > 0 ? th.max_path - 1 : 0;
-      // chunk length is independent of the window (the blocking algorithm
-      // runs one-position windows); a chunk should span at least its warm-up
-      const int64_t base = std::max<int64_t>(k.window, 2048);
-      int64_t chunk = k.chunk > 0 ? k.chunk : std::max<int64_t>(base - warm, base / 2);
-      chunk = std::max<int64_t>(chunk, 1);
-      for (int64_t em = slo; em < shi; em += chunk) {
-        UnitDev u;
-        u.tile = ti;
-        u.lo = std::max(slo, em - warm);
-        u.hi = std::min(em + chunk, shi);
-        u.emit_lo = em;
-        u.flags = (starts && u.lo == slo) ? 1u : 0u;
-        bounded.push_back(u);
-      }
-    }
-  }
+  units.insert(units.end(), unbounded.begin(), unbounded.end());
   const size_t nunb = units.size();
   units.insert(units.end(), bounded.begin(), bounded.end());
   const int64_t per_b = std::max<int64_t>(
@@ -362,6 +388,19 @@ void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vecto
   };
   cut(0, nunb, kWarpsPerCta);
   cut(nunb, units.size(), per_b);
+}
+
+void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vector<UnitDev>& units,
+                std::vector<TaskDev>& tasks) {
+  std::vector<UnitDev> unbounded, bounded;
+  for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
+    for (int64_t s = 0; s < k.num_seg; s++) {
+      SegSpec sp{s * k.seg_len, (s + 1) * k.seg_len, k.first_seg + s == 0 || k.is_dup != 0, 0ull,
+                 0};
+      add_units(t->tiles[ti], ti, sp, k.window, k.chunk, unbounded, bounded);
+    }
+  }
+  make_tasks(units, unbounded, bounded, grid, tasks);
 }
 
 __global__ void swap_halves(uint64_t* a, uint64_t n) {
@@ -429,6 +468,52 @@ int sort_unique(ngap_engine* e, uint64_t* d_in, const unsigned long long* d_n, u
   unique_write<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist, d_out);
   e->launches += 3;
   CUDA_TRY(cudaGetLastError());
+  return NGAP_OK;
+}
+
+// Batched keys stream << sshift | offset << oshift | id: radix passes over the
+// three fields, then unique reports and their stream indices.
+int sort_unique_fields(ngap_engine* e, const unsigned long long* d_n, uint64_t cap, int ibits,
+                       int oshift, int obits, int sshift, int sbits,
+                       unsigned long long* d_unique_n, cudaStream_t st) {
+  const uint32_t max_tiles = (uint32_t)((cap + kSortTile - 1) / kSortTile);
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, e->num_sms * 8));
+  std::vector<int> shifts;
+  for (int b = 0; b < ibits; b += 4) shifts.push_back(b);
+  for (int b = 0; b < obits; b += 4) shifts.push_back(oshift + b);
+  for (int b = 0; b < sbits; b += 4) shifts.push_back(sshift + b);
+  uint64_t* src = e->d_reports;
+  uint64_t* dst = e->d_tmp;
+  for (int sh : shifts) {
+    radix_hist<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, sh, e->d_hist);
+    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 16, nullptr);
+    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, d_n, cap, sh, e->d_hist);
+    e->launches += 3;
+    std::swap(src, dst);
+  }
+  unique_count<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist);
+  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 1, d_unique_n);
+  unique_write_fields<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist, oshift, sshift,
+                                                     e->d_unique, e->d_stream_ids);
+  e->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  return NGAP_OK;
+}
+
+// --algorithm -> prefix depth, privatization and window.
+int algo_config(int algo, int table_depth, int* depth, int* priv, int* window) {
+  switch (algo) {
+    case NGAP_ALGO_BLOCKING: *depth = 0; *window = 1; break;
+    case NGAP_ALGO_NAP: *depth = 0; break;
+    case NGAP_ALGO_NONBLOCKING: *depth = 1; break;
+    case NGAP_ALGO_NONBLOCKING_R1: *depth = 1; *priv = 1; break;
+    case NGAP_ALGO_NONBLOCKING_R2: *depth = 1; *priv = 2; break;
+    case NGAP_ALGO_NONBLOCKING_PC: *depth = std::max(1, table_depth); break;
+    case NGAP_ALGO_NONBLOCKING_ALL: *depth = std::max(1, table_depth); *priv = 1; break;
+    default:
+      set_error("not supported algoritm %d", algo);
+      return NGAP_E_INVALID;
+  }
   return NGAP_OK;
 }
 
@@ -530,6 +615,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     e->ntasks = (int32_t)tasks.size();
     e->plan_tables = t;
     e->plan_key = key;
+    e->batch_ts = nullptr;  // the batched plan cache no longer describes the buffers
   }
   const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
@@ -557,6 +643,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.active_threshold = p->active_threshold;
   mp.unique = p->unique;
   mp.report_off = p->report_off;
+  mp.off_shift = 32;
   mp.rep_count = e->d_counters + 0;
   mp.reports = e->d_reports;
   mp.rep_cap = cap;
@@ -682,6 +769,321 @@ int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, u
   CUDA_TRY(cudaMemcpyAsync(&un, e->d_counters + 6, sizeof(un), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   *n_out = un;
+  return NGAP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched matching: many streams, several NFAs, one persistent launch.
+// ---------------------------------------------------------------------------
+
+struct ngap_tableset {
+  std::vector<const ngap_tables*> tables;
+  std::vector<int> tile_base;  // first tile of each NFA in the combined descriptor array
+  TileDev* d_tiles = nullptr;
+  int ntiles = 0, image_region = 0, max_states = 0, max_groups = 1, max_depth = 1, device = 0;
+  ~ngap_tableset() { cudaFree(d_tiles); }
+};
+
+extern "C" {
+
+int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset** out) {
+  if (!tables || n <= 0 || !out) {
+    set_error("ngap_tableset_create: bad argument");
+    return NGAP_E_INVALID;
+  }
+  *out = nullptr;
+  std::unique_ptr<ngap_tableset> ts(new ngap_tableset());
+  std::vector<TileDev> all;
+  for (int i = 0; i < n; i++) {
+    const ngap_tables* t = tables[i];
+    if (!t || (i > 0 && t->device != tables[0]->device)) {
+      set_error("ngap_tableset_create: tables must exist and share one device");
+      return NGAP_E_INVALID;
+    }
+    ts->tables.push_back(t);
+    ts->tile_base.push_back((int)all.size());
+    all.insert(all.end(), t->dev_desc.begin(), t->dev_desc.end());
+    ts->image_region = std::max(ts->image_region, t->image_region);
+    ts->max_states = std::max(ts->max_states, t->max_states);
+    ts->max_groups = std::max(ts->max_groups, t->num_groups);
+    for (auto& th : t->tiles) ts->max_depth = std::max(ts->max_depth, th.depth);
+  }
+  ts->device = tables[0]->device;
+  ts->ntiles = (int)all.size();
+  CUDA_TRY(cudaSetDevice(ts->device));
+  if (!all.empty()) {
+    CUDA_TRY(cudaMalloc(&ts->d_tiles, all.size() * sizeof(TileDev)));
+    CUDA_TRY(cudaMemcpy(ts->d_tiles, all.data(), all.size() * sizeof(TileDev),
+                        cudaMemcpyHostToDevice));
+  }
+  *out = ts.release();
+  return NGAP_OK;
+}
+
+void ngap_tableset_destroy(ngap_tableset* ts) { delete ts; }
+
+int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* input,
+                     uint64_t input_bytes, int input_on_device, const ngap_batch_stream* streams,
+                     int nstreams, const ngap_batch_params* p, void* stream) {
+  if (!e || !ts || !p || !streams || nstreams <= 0 || (!input && input_bytes > 0)) {
+    set_error("ngap_batch_match: bad argument");
+    return NGAP_E_INVALID;
+  }
+  uint64_t max_len = 1;
+  for (int i = 0; i < nstreams; i++) {
+    const ngap_batch_stream& s = streams[i];
+    if (s.nfa < 0 || s.nfa >= (int)ts->tables.size() || s.offset + s.length > input_bytes) {
+      set_error("ngap_batch_match: stream %d is out of range", i);
+      return NGAP_E_INVALID;
+    }
+    max_len = std::max<uint64_t>(max_len, s.length + 1);
+  }
+  if (input_bytes >= (1ull << 32)) {
+    set_error("ngap_batch_match: batches are limited to 4 GiB of input");
+    return NGAP_E_UNSUPPORTED;
+  }
+  // report key: stream | offset in stream | id
+  const int ibits = 22 + bits_for((uint64_t)std::max(ts->max_groups, 1));
+  const int obits = bits_for(max_len);
+  const int sbits = bits_for((uint64_t)nstreams);
+  const int oshift = ibits, sshift = ibits + obits;
+  if (sshift + sbits > 64) {
+    set_error("ngap_batch_match: stream count, stream length and group count exceed a 64-bit key");
+    return NGAP_E_UNSUPPORTED;
+  }
+  CUDA_TRY(cudaSetDevice(e->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  e->stream = st;
+  e->ran = false;
+  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 1024;
+  int rc = algo_config(p->algorithm, ts->max_depth, &depth, &priv, &window);
+  if (rc != NGAP_OK) return rc;
+  window = std::min(window, kMaxWindow);
+  while (window > 64 && cta_smem_bytes(window, ts->image_region) > 227 * 1024 - 1024) window /= 2;
+  const int smem = cta_smem_bytes(window, ts->image_region);
+  if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
+  int bps = 0;
+  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
+                                                              : blocks_per_sm<2>(smem, &bps);
+  if (rc != NGAP_OK) return rc;
+  const int full_grid = e->num_sms * bps;
+  // buffers (before any capture)
+  size_t need = ((input_bytes + 15) & ~(uint64_t)15) + 64;
+  if (need > e->input_cap) {
+    cudaFree(e->d_input);
+    e->d_input = nullptr;
+    e->input_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_input, need));
+    e->input_cap = need;
+  }
+  const uint64_t cap = p->result_capacity > 0 ? p->result_capacity : 54619400ull;
+  if ((rc = ensure_reports(e, cap)) != NGAP_OK) return rc;
+  if (cap > e->stream_ids_cap) {
+    cudaFree(e->d_stream_ids);
+    e->d_stream_ids = nullptr;
+    e->stream_ids_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_stream_ids, cap * sizeof(uint32_t)));
+    e->stream_ids_cap = cap;
+  }
+  // plan: tiles outer (tasks share a staged image), streams of the tile's NFA inner
+  const std::vector<ngap_batch_stream> sv(streams, streams + nstreams);
+  auto same_streams = [&]() {
+    if (e->batch_streams.size() != sv.size()) return false;
+    for (size_t i = 0; i < sv.size(); i++)
+      if (sv[i].offset != e->batch_streams[i].offset || sv[i].length != e->batch_streams[i].length ||
+          sv[i].nfa != e->batch_streams[i].nfa)
+        return false;
+    return true;
+  };
+  bool replanned = false;
+  if (e->batch_ts != ts || e->batch_window != window || e->batch_chunk != p->chunk ||
+      !same_streams() || e->plan_tables != nullptr) {
+    std::vector<std::vector<int>> by_nfa(ts->tables.size());
+    for (int i = 0; i < nstreams; i++) by_nfa[sv[i].nfa].push_back(i);
+    std::vector<UnitDev> unbounded, bounded, units;
+    std::vector<TaskDev> tasks;
+    for (size_t n = 0; n < ts->tables.size(); n++) {
+      const ngap_tables* t = ts->tables[n];
+      for (int ti = 0; ti < (int)t->tiles.size(); ti++)
+        for (int si : by_nfa[n]) {
+          const ngap_batch_stream& s = sv[si];
+          if (s.length == 0) continue;
+          SegSpec sp{(int64_t)s.offset, (int64_t)(s.offset + s.length), true,
+                     (uint64_t)si << sshift, (int64_t)s.offset};
+          add_units(t->tiles[ti], ts->tile_base[n] + ti, sp, window, p->chunk, unbounded, bounded);
+        }
+    }
+    make_tasks(units, unbounded, bounded, full_grid, tasks);
+    if (units.size() > e->units_cap) {
+      cudaFree(e->d_units);
+      e->d_units = nullptr;
+      e->units_cap = 0;
+      CUDA_TRY(cudaMalloc(&e->d_units, units.size() * sizeof(UnitDev)));
+      e->units_cap = units.size();
+    }
+    if (tasks.size() > e->tasks_cap) {
+      cudaFree(e->d_tasks);
+      e->d_tasks = nullptr;
+      e->tasks_cap = 0;
+      CUDA_TRY(cudaMalloc(&e->d_tasks, tasks.size() * sizeof(TaskDev)));
+      e->tasks_cap = tasks.size();
+    }
+    if (!units.empty())
+      CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
+                          cudaMemcpyHostToDevice));
+    if (!tasks.empty())
+      CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
+                          cudaMemcpyHostToDevice));
+    e->nunits = (int32_t)units.size();
+    e->ntasks = (int32_t)tasks.size();
+    e->plan_tables = nullptr;  // the plain plan cache no longer describes the buffers
+    e->plan_key = UnitPlanKey{-1, -1, -1, -1, -1, -1};
+    e->batch_ts = ts;
+    e->batch_streams = sv;
+    e->batch_window = window;
+    e->batch_chunk = p->chunk;
+    replanned = true;
+  }
+  const int grid = std::max(1, std::min(full_grid, e->ntasks));
+  e->grid = grid;
+  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states)) != NGAP_OK) return rc;
+
+  MatchParams mp;
+  mp.tiles = ts->d_tiles;
+  mp.units = e->d_units;
+  mp.tasks = e->d_tasks;
+  mp.ntasks = e->ntasks;
+  mp.image_region = ts->image_region;
+  mp.input = e->d_input;
+  mp.window = window;
+  mp.depth = depth;
+  mp.active_threshold = p->active_threshold;
+  mp.unique = p->unique;
+  mp.report_off = p->report_off;
+  mp.off_shift = oshift;
+  mp.rep_count = e->d_counters + 0;
+  mp.reports = e->d_reports;
+  mp.rep_cap = cap;
+  mp.err = e->d_err;
+  mp.task_counter = e->d_unit_counter;
+  mp.carry = e->d_carry;
+  mp.marks = e->d_marks;
+  mp.ovf = e->d_ovf;
+  mp.carry_cap = e->carry_cap;
+  mp.mark_words = e->mark_words;
+  mp.ovf_cap = e->ovf_cap;
+  mp.work = e->d_counters + 2;
+
+  auto enqueue = [&](cudaStream_t qs) -> int {
+    if (input_on_device)
+      CUDA_TRY(cudaMemcpyAsync(e->d_input, input, input_bytes, cudaMemcpyDeviceToDevice, qs));
+    else
+      CUDA_TRY(cudaMemcpyAsync(e->d_input, input, input_bytes, cudaMemcpyHostToDevice, qs));
+    CUDA_TRY(cudaMemsetAsync(e->d_counters, 0, 8 * sizeof(unsigned long long), qs));
+    CUDA_TRY(cudaMemsetAsync(e->d_err, 0, sizeof(int), qs));
+    CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, sizeof(unsigned int), qs));
+    int r = NGAP_OK;
+    if (e->ntasks > 0) {
+      r = priv == 0 ? launch_match<0>(e, mp, smem, qs)
+                    : priv == 1 ? launch_match<1>(e, mp, smem, qs) : launch_match<2>(e, mp, smem, qs);
+      if (r != NGAP_OK) return r;
+      e->launches++;
+    }
+    if (!p->report_off) {
+      r = sort_unique_fields(e, e->d_counters + 0, cap, ibits, oshift, obits, sshift, sbits,
+                             e->d_counters + 1, qs);
+      if (r != NGAP_OK) return r;
+    }
+    CUDA_TRY(cudaMemcpyAsync(e->h_counters, e->d_counters, 4 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, qs));
+    CUDA_TRY(cudaMemcpyAsync(e->h_counters + 4, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, qs));
+    return NGAP_OK;
+  };
+
+  e->launches = 0;
+  if (!p->use_graph) {
+    e->graph_mode = false;
+    CUDA_TRY(cudaEventRecord(e->ev[0], st));
+    CUDA_TRY(cudaEventRecord(e->ev[1], st));
+    if ((rc = enqueue(st)) != NGAP_OK) return rc;
+    CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    CUDA_TRY(cudaEventRecord(e->ev[3], st));
+    e->ran = true;
+    return NGAP_OK;
+  }
+  // CUDA graph: the same tableset, streams, parameters and input pointer replay
+  // one captured pipeline (copy, match, sort, unique, counters). Capture and
+  // replay use the engine's own stream (the legacy default stream cannot be
+  // captured), ordered after and before the caller's stream by events.
+  if (!e->cap_stream) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->cap_ev[0], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->cap_ev[1], cudaEventDisableTiming));
+  }
+  cudaStream_t cs = e->cap_stream;
+  std::vector<uint64_t> key = {(uint64_t)(uintptr_t)ts, (uint64_t)(uintptr_t)input, input_bytes,
+                               (uint64_t)input_on_device, (uint64_t)p->algorithm,
+                               (uint64_t)p->unique, (uint64_t)p->active_threshold,
+                               (uint64_t)p->report_off, cap, (uint64_t)window, (uint64_t)p->chunk};
+  if (replanned || !e->graph || key != e->graph_key) {
+    if (e->graph) {
+      cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue(cs);
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    if (rc != NGAP_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) {
+      set_error("CUDA graph capture failed: %s", cudaGetErrorString(ce));
+      return NGAP_E_CUDA;
+    }
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      e->graph = nullptr;
+      set_error("CUDA graph instantiation failed: %s", cudaGetErrorString(ce));
+      return NGAP_E_CUDA;
+    }
+    e->graph_key = key;
+    e->graph_launches = e->launches;
+  }
+  e->graph_mode = true;
+  e->launches = e->graph_launches;
+  CUDA_TRY(cudaEventRecord(e->cap_ev[0], st));  // after the caller's prior work
+  CUDA_TRY(cudaStreamWaitEvent(cs, e->cap_ev[0], 0));
+  CUDA_TRY(cudaEventRecord(e->ev[0], cs));
+  CUDA_TRY(cudaEventRecord(e->ev[1], cs));
+  CUDA_TRY(cudaGraphLaunch(e->graph, cs));
+  CUDA_TRY(cudaEventRecord(e->ev[2], cs));
+  CUDA_TRY(cudaEventRecord(e->ev[3], cs));
+  CUDA_TRY(cudaEventRecord(e->cap_ev[1], cs));  // the caller's later work waits for the graph
+  CUDA_TRY(cudaStreamWaitEvent(st, e->cap_ev[1], 0));
+  e->stream = cs;
+  e->ran = true;
+  return NGAP_OK;
+}
+
+int ngap_batch_results(ngap_engine* e, uint64_t* reports, uint32_t* stream_ids, uint64_t cap,
+                       uint64_t* n) {
+  if (!e || !reports || !n) {
+    set_error("ngap_batch_results: null argument");
+    return NGAP_E_INVALID;
+  }
+  const uint64_t k = std::min<uint64_t>(e->h_counters[1], cap);
+  *n = 0;
+  if (k == 0) return NGAP_OK;
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemcpy(reports, e->d_unique, k * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (stream_ids)
+    CUDA_TRY(cudaMemcpy(stream_ids, e->d_stream_ids, k * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  *n = k;
   return NGAP_OK;
 }
 

@@ -63,6 +63,7 @@ struct MatchParams {
   int32_t active_threshold; // privatize when more lanes than this expand
   int32_t unique;
   int32_t report_off;
+  int32_t off_shift;        // bit position of the offset in report keys (32 when not batched)
   unsigned long long* rep_count;
   uint64_t* reports;        // key = offset << 32 | id
   uint64_t rep_cap;
@@ -99,6 +100,8 @@ struct WarpRun {
   int ovf_n;   // overflow stack size
   int ncarry;  // carry entries for the next window
   int nrep;    // buffered reports
+  uint32_t base;                // current unit's stream start (low 32 bits of positions)
+  unsigned long long key_hi;    // current unit's stream index in the report key
   uint32_t* ovf;
   uint32_t* carry;
   uint32_t* marks;
@@ -222,7 +225,9 @@ __device__ __forceinline__ void emit_report(const MatchParams& p, WarpSmem& ws, 
   if (m == 0) return;
   const int cnt = __popc(m);
   if (w.nrep + cnt > kReportBuf) flush_reports(p, ws, w, lane);
-  if (pred) ws.rbuf[w.nrep + __popc(m & lanemask_lt(lane))] = ((unsigned long long)off << 32) | id;
+  if (pred)
+    ws.rbuf[w.nrep + __popc(m & lanemask_lt(lane))] =
+        w.key_hi | ((unsigned long long)(off - w.base) << p.off_shift) | id;
   w.nrep += cnt;
   __syncwarp();
 }
@@ -534,6 +539,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   const int slot = blockIdx.x * kWarpsPerCta + warp;
   WarpRun w;
   w.top = w.ovf_n = w.ncarry = w.nrep = 0;
+  w.base = 0;
+  w.key_hi = 0ull;
   w.ovf = p.ovf + (size_t)slot * p.ovf_cap;
   w.carry = p.carry + (size_t)slot * p.carry_cap;
   w.marks = p.marks + (size_t)slot * p.mark_words;
@@ -609,6 +616,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       UnitCtx c;
       c.hi = un.hi;
       c.emit_lo = un.emit_lo;
+      w.key_hi = un.key_hi;
+      w.base = (uint32_t)un.base;
       int cur = 0;
       uint32_t nbytes[2];
       nbytes[0] = issue(0, un.lo, c.hi);

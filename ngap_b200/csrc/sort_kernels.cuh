@@ -216,4 +216,51 @@ __global__ void __launch_bounds__(kSortThreads) unique_write(const uint64_t* __r
   }
 }
 
+// Batched form of unique_write: keys are stream << sshift | offset << oshift |
+// id; writes the reference encoding (id << 32 | offset, offset local to the
+// stream) and the stream index of each unique report.
+__global__ void __launch_bounds__(kSortThreads) unique_write_fields(
+    const uint64_t* __restrict__ keys, const unsigned long long* d_n, uint64_t cap,
+    const uint32_t* __restrict__ offs, int oshift, int sshift, uint64_t* __restrict__ out,
+    uint32_t* __restrict__ out_stream) {
+  __shared__ uint32_t wsum[kSortThreads / 32];
+  const uint64_t n = dev_count(d_n, cap);
+  const uint32_t ntiles = num_tiles(n);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint64_t id_mask = (1ull << oshift) - 1, off_mask = (1ull << (sshift - oshift)) - 1;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint64_t base = (uint64_t)tile * kSortTile;
+    uint32_t flags = 0, c = 0;
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+      uint64_t g = base + (uint64_t)t * kSortItems + k;
+      bool f = g < n && (g == 0 || keys[g] != keys[g - 1]);
+      flags |= (uint32_t)f << k;
+      c += f;
+    }
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int i = 0; i < warp; i++) before += wsum[i];
+    uint32_t pos = offs[tile] + before + incl - c;
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+      if (flags & (1u << k)) {
+        const uint64_t key = keys[base + (uint64_t)t * kSortItems + k];
+        const uint64_t id = key & id_mask, off = (key >> oshift) & off_mask;
+        out[pos] = (id << 32) | off;
+        out_stream[pos] = sshift < 64 ? (uint32_t)(key >> sshift) : 0u;
+        pos++;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace ngap

@@ -220,6 +220,69 @@ class Engine:
             self._h = ctypes.c_void_p()
 
 
+class TableSet:
+    """Tables of several NFAs usable in one batched launch."""
+
+    def __init__(self, tables):
+        self.tables = list(tables)  # keep them alive
+        arr = (ctypes.c_void_p * len(self.tables))(*[t._h.value for t in self.tables])
+        h = ctypes.c_void_p()
+        check(lib().ngap_tableset_create(arr, len(self.tables), ctypes.byref(h)))
+        self._h = h
+
+    def __len__(self):
+        return len(self.tables)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
+            _lib._lib.ngap_tableset_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+def batch_match_async(engine, tableset, data, offsets, lengths, nfas,
+                      algorithm="nonblockingpcgroups", unique=False, active_threshold=20,
+                      report_off=False, result_capacity=54619400, window=0, chunk=0,
+                      use_graph=False, stream=None):
+    """Starts one launch over all streams: stream i is data[offsets[i] :
+    offsets[i] + lengths[i]] matched against tableset NFA nfas[i]. `data` is a
+    numpy uint8 array (pinned memory is needed with use_graph) or a CUDA tensor."""
+    n = len(offsets)
+    ss = (_lib.BatchStream * n)()
+    for i in range(n):
+        ss[i] = _lib.BatchStream(int(offsets[i]), int(lengths[i]), int(nfas[i]), 0)
+    engine._keep_streams = ss
+    algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+    p = _lib.BatchParams(algo, int(unique), active_threshold, int(report_off), result_capacity,
+                         window, chunk, int(use_graph))
+    if hasattr(data, "data_ptr"):
+        ptr, on_dev, nbytes = data.data_ptr(), int(getattr(data, "is_cuda", True)), data.numel()
+    else:
+        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        engine._keep = arr
+        ptr, on_dev, nbytes = arr.ctypes.data, 0, arr.nbytes
+    check(lib().ngap_batch_match(engine._h, tableset._h, ctypes.c_void_p(ptr), nbytes, on_dev, ss,
+                                 n, ctypes.byref(p), ctypes.c_void_p(stream or 0)))
+
+
+def batch_results(engine):
+    """(reports, stream_ids): unique reports sorted by (stream, offset, id);
+    offsets are local to each stream."""
+    _, n = engine.counts()
+    rep = np.zeros(n, dtype=np.uint64)
+    sid = np.zeros(n, dtype=np.uint32)
+    got = ctypes.c_uint64()
+    if n:
+        check(lib().ngap_batch_results(engine._h, rep.ctypes.data, sid.ctypes.data, n,
+                                       ctypes.byref(got)))
+    return rep[:got.value], sid[:got.value]
+
+
+def split_by_stream(reports, stream_ids, nstreams):
+    """List of per-stream report arrays."""
+    bounds = np.searchsorted(stream_ids, np.arange(nstreams + 1, dtype=np.uint32))
+    return [reports[bounds[i]:bounds[i + 1]] for i in range(nstreams)]
+
+
 def cpu_validate(groups, data, num_seg, seg_len, is_dup=False):
     """The library's CPU checker (the CLI's --validation): sorted unique reports."""
     arr = np.ascontiguousarray(data, dtype=np.uint8)

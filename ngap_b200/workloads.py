@@ -244,6 +244,69 @@ def high_frontier(seed=3, n_lev=500, n_dot=2000, half=16 << 20):
     return w.text(), np.concatenate([dna, asc])
 
 
+def batched_suite(seed=4, n_nfas=16, n_streams=4096, min_states=2000, max_states=200000,
+                  len_lo=1 << 10, len_hi=4 << 20, sample_len=1 << 16):
+    """Several NFAs and many streams of uneven length.
+
+    NFA i has a size drawn log-uniformly in [min_states, max_states] STEs and
+    comes from the literal, Hamming, Levenshtein and dot-star generators in
+    turn. Stream lengths are log-uniform in [len_lo, len_hi]; each stream gets
+    an NFA uniformly at random and, by seed, either the NFA generator's own
+    input law with planted occurrences (a random rotation of a sample), or
+    fresh bytes over the NFA's alphabet (ACGT or printable ASCII) drawn
+    uniformly or from a Zipf(1.1) law.
+
+    Returns (nfas, data, offsets, lengths, nfa_of): nfas is a list of dicts
+    (kind, anml, states_hint), data the concatenated streams.
+    """
+    rng = np.random.default_rng(seed)
+    per_pattern = {"literal": 12, "hamming": 166, "levenshtein": 135, "dotstar": 17}
+    kinds = ["literal", "hamming", "levenshtein", "dotstar"]
+    nfas, samples = [], []
+    for i in range(n_nfas):
+        kind = kinds[i % 4]
+        target = int(np.exp(rng.uniform(np.log(min_states), np.log(max_states))))
+        n = max(1, target // per_pattern[kind])
+        sub = int(rng.integers(1 << 30))
+        if kind == "literal":
+            anml, sample = literal_set(seed=sub, n_patterns=n, input_len=sample_len,
+                                       plant_every=1 << 9)
+        elif kind == "hamming":
+            anml, sample = hamming_set(seed=sub, n_patterns=n, input_len=sample_len,
+                                       plant_every=1 << 10)
+        elif kind == "levenshtein":
+            anml, sample = levenshtein_set(seed=sub, n_patterns=n, input_len=sample_len,
+                                           plant_every=1 << 10)
+        else:
+            anml, sample = dotstar_set(seed=sub, n_patterns=n, input_len=sample_len,
+                                       plant_every=1 << 10)
+        nfas.append({"kind": kind, "anml": anml, "states_hint": n * per_pattern[kind]})
+        samples.append(sample)
+    lengths = np.exp(rng.uniform(np.log(len_lo), np.log(len_hi), size=n_streams)).astype(np.int64)
+    nfa_of = rng.integers(0, n_nfas, size=n_streams)
+    law = rng.integers(0, 3, size=n_streams)  # 0 generator sample, 1 uniform, 2 Zipf
+    offsets = np.zeros(n_streams, dtype=np.int64)
+    offsets[1:] = np.cumsum(lengths)[:-1]
+    data = np.empty(int(lengths.sum()), dtype=np.uint8)
+    for s in range(n_streams):
+        L, k = int(lengths[s]), int(nfa_of[s])
+        out = data[offsets[s]:offsets[s] + L]
+        dna = nfas[k]["kind"] in ("hamming", "levenshtein")
+        alpha = ACGT if dna else PRINTABLE
+        if law[s] == 0:
+            smp = samples[k]
+            rot = int(rng.integers(len(smp)))
+            out[:] = np.resize(np.roll(smp, -rot), L)
+        elif law[s] == 1:
+            out[:] = alpha[rng.integers(0, len(alpha), size=L)]
+        else:
+            ranks = np.arange(1, len(alpha) + 1, dtype=np.float64) ** -1.1
+            cdf = np.cumsum(ranks / ranks.sum())
+            perm = rng.permutation(alpha)
+            out[:] = perm[np.minimum(np.searchsorted(cdf, rng.random(L)), len(alpha) - 1)]
+    return nfas, data, offsets, lengths, nfa_of
+
+
 CONFIGS = {
     "literal_set": literal_set,
     "hamming_set": hamming_set,
