@@ -65,6 +65,8 @@ struct TileDev {
   int32_t image_bytes = 0;  // multiple of 16
   int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
   int32_t inj_batch = 32;   // positions injected per worklist refill
+  int32_t nsticky = 0;      // sticky states (bitmap at off_sticky in the image)
+  int32_t off_sticky = 0;
   const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
   const uint32_t* sid = nullptr;    // [nstates] local -> group-local sid
   const uint32_t* aas = nullptr;    // [naas] local ids

@@ -205,6 +205,8 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.off_rep = th.off_rep;
     d.off_cls = th.off_cls;
     d.inj_batch = th.inj_batch;
+    d.nsticky = th.nsticky;
+    d.off_sticky = th.off_sticky;
     if ((rc = t->upload(th.image, &d.image)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.sid, &d.sid)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.aas, &d.aas)) != NGAP_OK) return rc;

@@ -41,6 +41,8 @@ constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr int kStackCap = 512;    // entries per warp in shared memory
 constexpr int kReportBuf = 64;    // reports per warp buffered in shared memory
 constexpr int kInjectLow = 256;   // inject new positions while the stack holds fewer entries
+constexpr int kStickyCap = 64;    // sticky states tracked per warp (more fall back to entries)
+constexpr int kPendCap = 16;      // sticky states met while copying one injection batch
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNoEntry = 0xffffffffu;  // never a valid entry: offsets stay < 8191
 constexpr uint32_t kIdMask = 0x7fffffffu;
@@ -79,7 +81,8 @@ struct MatchParams {
 __host__ __device__ inline int window_buf_bytes(int W) { return ((W + 48) + 15) & ~15; }
 
 __host__ __device__ inline int warp_smem_bytes(int W) {
-  return kStackCap * 4 + 2 * window_buf_bytes(W) + kReportBuf * 8 + 3 * 32 * 4 + 16;
+  return kStackCap * 4 + 2 * window_buf_bytes(W) + kReportBuf * 8 + 3 * 32 * 4 + 16 +
+         kStickyCap * 8 + kPendCap * 8 + 16;
 }
 
 __host__ __device__ inline int cta_smem_bytes(int W, int image_region) {
@@ -92,6 +95,11 @@ struct WarpSmem {
   unsigned long long* rbuf;  // kReportBuf
   uint32_t* inj;             // 3 x 32 words of injection scratch
   uint64_t* bar;             // 2 mbarriers
+  uint32_t* stk_s;           // kStickyCap sticky states active in the unit
+  uint32_t* stk_q;           //   and the position of their first match (low 32 bits)
+  uint32_t* pend_s;          // kPendCap sticky states met while copying a batch
+  uint32_t* pend_q;
+  uint32_t* pend_n;          // count (one word)
 };
 
 // Per-warp state kept in registers (uniform across the warp).
@@ -100,6 +108,7 @@ struct WarpRun {
   int ovf_n;   // overflow stack size
   int ncarry;  // carry entries for the next window
   int nrep;    // buffered reports
+  int nstk;    // sticky states active in the unit
   uint32_t base;                // current unit's stream start (low 32 bits of positions)
   unsigned long long key_hi;    // current unit's stream index in the report key
   uint32_t* ovf;
@@ -114,6 +123,7 @@ struct TileView {
   const uint2* succ2;   // narrow tiles: 4 x u16
   const uint32_t* cmask;
   const uint32_t* rep;
+  const uint32_t* sticky;  // sticky-state bitmap, nullptr when the tile has none
   const uint8_t* cls;
   const TileDev* t;
   const PrefixTableDev* pt;  // the tile's prefix tables (shared-memory copy)
@@ -315,10 +325,127 @@ __device__ __forceinline__ void pt_find(const PrefixTableDev& t, uint32_t key, b
   }
 }
 
+// Reports (slow path, taken only when some lane has one) for up to 4 matched
+// states u[j] (bit 31 = report flag) at stream position q.
+__device__ __forceinline__ void report4(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                        const TileView& tv, int lane, const bool ok[4],
+                                        const uint32_t u[4], int64_t q, bool in_range) {
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < 4; j++) any |= ok[j] && (u[j] >> 31);
+  if (!__any_sync(kFull, any && in_range)) return;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const bool rep = in_range && ok[j] && (u[j] >> 31);
+    emit_report(p, ws, w, lane, rep, rep ? (__ldg(tv.t->sid + (u[j] & kIdMask)) | tv.gbits) : 0u,
+                (uint32_t)q);
+  }
+}
+
+// ---- sticky states ----------------------------------------------------------
+// A sticky state (not always-active, a self-loop, every byte accepted) that
+// matches at position q matches again at every later position of the segment,
+// so from q on it acts like an always-active state. Instead of a chain of
+// worklist entries advancing one position per step, a warp keeps the unit's
+// active sticky states in a small shared list with their first match; the
+// injection of each position adds their work, and a state registered late
+// catches up the positions already injected.
+
+__device__ __forceinline__ bool is_sticky(const TileView& tv, uint32_t v) {
+  return (tv.sticky[v >> 5] >> (v & 31)) & 1u;
+}
+
+// Work of active sticky state s at stream position t (act: s matched at t - 1):
+// its own report at t, and its other successors tested against the symbol at
+// t. Warp-collective.
+__device__ __forceinline__ void sticky_at(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                          const TileView& tv, const UnitCtx& c, int lane,
+                                          uint32_t s, const uint32_t us[4], bool srep, bool act,
+                                          int64_t t) {
+  const int r = (int)(t - c.wb);
+  const uint32_t sym = act ? c.in[r] : 0u;
+  const bool rs = act && srep && t >= c.emit_lo;
+  emit_report(p, ws, w, lane, rs, rs ? (__ldg(tv.t->sid + s) | tv.gbits) : 0u, (uint32_t)t);
+  bool ok[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    ok[j] = act && us[j] != kNoSucc && (us[j] & kIdMask) != s && accepts(tv, us[j] & kIdMask, sym);
+  report4(p, ws, w, tv, lane, ok, us, t, t >= c.emit_lo);
+  const bool need = act && t + 1 < c.hi;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    push_entry(p, ws, w, lane, need && ok[j], ((us[j] & kIdMask) << kEntryPosBits) | (uint32_t)r);
+}
+
+// Sticky state s's work over positions [t0, t1), lanes over positions.
+__device__ __forceinline__ void sticky_span(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                         const TileView& tv, const UnitCtx& c, int lane, uint32_t s,
+                                         int64_t t0, int64_t t1) {
+  const uint4 sc = load_succ(tv, s);
+  const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+  const bool srep = is_report(tv, s);
+  for (int64_t tb = t0; tb < t1; tb += 32) {
+    const int64_t t = tb + lane;
+    sticky_at(p, ws, w, tv, c, lane, s, us, srep, t < t1, t);
+  }
+}
+
+// Warp-uniform: sticky state s matched at q. Positions below inj_end have been
+// injected already and are caught up here; later ones are handled by
+// injection. Returns false when the list is full (the caller keeps an entry).
+__device__ __forceinline__ bool register_sticky(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                             const TileView& tv, const UnitCtx& c, int lane,
+                                             uint32_t s, int64_t q, int64_t inj_end) {
+  int found = -1;
+  for (int i0 = 0; i0 < w.nstk && found < 0; i0 += 32) {
+    const int i = i0 + lane;
+    const unsigned m = __ballot_sync(kFull, i < w.nstk && ws.stk_s[i] == s);
+    if (m) found = i0 + __ffs(m) - 1;
+  }
+  int64_t t1;
+  if (found >= 0) {
+    const int64_t old = (int64_t)ws.stk_q[found];
+    if (q >= old) return true;  // already active from an earlier position
+    t1 = min(old + 1, inj_end);
+    __syncwarp();
+    if (lane == 0) ws.stk_q[found] = (uint32_t)q;
+  } else {
+    if (w.nstk >= kStickyCap) return false;
+    if (lane == 0) {
+      ws.stk_s[w.nstk] = s;
+      ws.stk_q[w.nstk] = (uint32_t)q;
+    }
+    w.nstk++;
+    t1 = inj_end;
+  }
+  __syncwarp();
+  t1 = min(t1, c.hi);
+  if (q + 1 < t1) sticky_span(p, ws, w, tv, c, lane, s, q + 1, t1);
+  return true;
+}
+
+// Registers the sticky states of all predicated lanes; true on lanes whose
+// state was registered (those need no worklist entry).
+__device__ __forceinline__ bool register_each(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                              const TileView& tv, const UnitCtx& c, int lane,
+                                              bool pred, uint32_t s, int64_t q, int64_t inj_end) {
+  unsigned m = __ballot_sync(kFull, pred);
+  bool mine = false;
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    const uint32_t ss = __shfl_sync(kFull, s, src);
+    const long long qq = __shfl_sync(kFull, (long long)q, src);
+    const bool ok = register_sticky(p, ws, w, tv, c, lane, ss, (int64_t)qq, inj_end);
+    if (lane == src) mine = ok;
+  }
+  return mine;
+}
+
 // Always-active states for window offsets [r0, r0 + batch) (one per lane).
-__device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpRun& w,
-                                       const TileView& tv, const UnitCtx& c, int lane, int r0,
-                                       int batch, int depth, unsigned long long& n_injected) {
+__device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                           const TileView& tv, const UnitCtx& c, int lane, int r0,
+                                           int batch, int depth, unsigned long long& n_injected) {
   const TileDev& t = *tv.t;
   const int r = r0 + lane;
   const bool valid = lane < batch && r < c.wlen;
@@ -392,34 +519,117 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
     const uint32_t before = l0 > 0 ? ws.inj[l0 - 1] : 0u;
     const int kk = (int)ws.inj[64 + l0];
     const uint32_t v = __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
-    store_entry(p, ws, w, w.top + (int)idx, (v << kEntryPosBits) | (uint32_t)(r0 + l0 + kk - 1));
+    const uint32_t off = (uint32_t)(r0 + l0 + kk - 1);
+    uint32_t e = (v << kEntryPosBits) | off;
+    if (tv.sticky && is_sticky(tv, v)) {  // registered after the copy instead
+      const uint32_t slot = atomicAdd(ws.pend_n, 1u);
+      if (slot < (uint32_t)kPendCap) {
+        ws.pend_s[slot] = v;
+        ws.pend_q[slot] = (uint32_t)(c.wb + off);
+        e = kNoEntry;
+      }
+    }
+    store_entry(p, ws, w, w.top + (int)idx, e);
   }
   grow_stack(p, w, (int)total);
   __syncwarp();
 }
 
-// Reports (slow path, taken only when some lane has one) for up to 4 matched
-// states u[j] (bit 31 = report flag) at stream position q.
-__device__ __forceinline__ void report4(const MatchParams& p, WarpSmem& ws, WarpRun& w,
-                                        const TileView& tv, int lane, const bool ok[4],
-                                        const uint32_t u[4], int64_t q, bool in_range) {
-  bool any = false;
-#pragma unroll
-  for (int j = 0; j < 4; j++) any |= ok[j] && (u[j] >> 31);
-  if (!__any_sync(kFull, any && in_range)) return;
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const bool rep = in_range && ok[j] && (u[j] >> 31);
-    emit_report(p, ws, w, lane, rep, rep ? (__ldg(tv.t->sid + (u[j] & kIdMask)) | tv.gbits) : 0u,
-                (uint32_t)q);
+// Injection of a batch of positions: always-active states, then the sticky
+// states met while copying, then the work of every active sticky state at
+// these positions.
+__device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                       const TileView& tv, const UnitCtx& c, int lane, int r0,
+                                       int batch, int depth, unsigned long long& n_injected) {
+  inject_aas(p, ws, w, tv, c, lane, r0, batch, depth, n_injected);
+  if (!tv.sticky) return;
+  __syncwarp();
+  const int np = min((int)*ws.pend_n, kPendCap);
+  for (int i = 0; i < np; i++) {
+    const uint32_t s = ws.pend_s[i];
+    const int64_t qq = (int64_t)ws.pend_q[i];
+    const bool ok = register_sticky(p, ws, w, tv, c, lane, s, qq, c.wb + r0);
+    push_entry(p, ws, w, lane, !ok && lane == 0 && qq + 1 < c.hi,
+               (s << kEntryPosBits) | (uint32_t)(qq - c.wb));
   }
+  __syncwarp();
+  if (lane == 0) *ws.pend_n = 0u;
+  __syncwarp();
+  if (w.nstk == 0) return;
+  // every active sticky state at this batch's positions (lanes over positions):
+  // count the successors that match, one prefix sum, write; reports (rare)
+  // through the warp-collective path
+  const int r = r0 + lane;
+  const bool valid = lane < batch && r < c.wlen;
+  const int64_t t = c.wb + r;
+  const uint32_t sym = valid ? c.in[r] : 0u;
+  const bool need = valid && t + 1 < c.hi;
+  int cnt = 0;
+  bool any_rep = false;
+  for (int i = 0; i < w.nstk; i++) {
+    const uint32_t s = ws.stk_s[i];
+    if (!(valid && t > (int64_t)ws.stk_q[i])) continue;
+    any_rep |= is_report(tv, s) && t >= c.emit_lo;
+    const uint4 sc = load_succ(tv, s);
+    const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t u = us[j] & kIdMask;
+      if (us[j] != kNoSucc && u != s && accepts(tv, u, sym)) {
+        cnt++;
+        any_rep |= (us[j] >> 31) && t >= c.emit_lo;
+      }
+    }
+  }
+  if (__any_sync(kFull, any_rep)) {
+    for (int i = 0; i < w.nstk; i++) {
+      const uint32_t s = ws.stk_s[i];
+      const bool act = valid && t > (int64_t)ws.stk_q[i];
+      const bool rs = act && is_report(tv, s) && t >= c.emit_lo;
+      emit_report(p, ws, w, lane, rs, rs ? (__ldg(tv.t->sid + s) | tv.gbits) : 0u, (uint32_t)t);
+      const uint4 sc = load_succ(tv, s);
+      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+      bool ok[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        ok[j] = act && us[j] != kNoSucc && (us[j] & kIdMask) != s &&
+                accepts(tv, us[j] & kIdMask, sym);
+      report4(p, ws, w, tv, lane, ok, us, t, t >= c.emit_lo);
+    }
+  }
+  const int pc = need ? cnt : 0;
+  int incl = pc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  if (pc) {
+    int pos = w.top + incl - pc;
+    for (int i = 0; i < w.nstk; i++) {
+      const uint32_t s = ws.stk_s[i];
+      if (t <= (int64_t)ws.stk_q[i]) continue;
+      const uint4 sc = load_succ(tv, s);
+      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t u = us[j] & kIdMask;
+        if (us[j] != kNoSucc && u != s && accepts(tv, u, sym))
+          store_entry(p, ws, w, pos++, (u << kEntryPosBits) | (uint32_t)r);
+      }
+    }
+  }
+  grow_stack(p, w, total);
+  __syncwarp();
 }
 
 // Expands the up-to-32 entries on top of the stack: one step of the worklist.
 template <int PRIV>
 __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, WarpRun& w,
                                             const TileView& tv, const UnitCtx& c, int lane,
-                                            unsigned long long& n_expanded) {
+                                            int cursor, unsigned long long& n_expanded) {
   const int n = min(w.top, 32);
   uint32_t e = lane < n ? ws.stack[w.top - 1 - lane] : kNoEntry;
   w.top -= n;
@@ -450,12 +660,24 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
   report4(p, ws, w, tv, lane, ok, u, q + 1, q + 1 >= c.emit_lo);
   const bool need = go && q + 2 < c.hi;        // the successors have a next symbol
   const bool at_end = r + 1 == c.wlen;         // successors sit at the next window's start
+  if (tv.sticky) {  // matched sticky states are registered instead of pushed
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const bool stk = ok[j] && need && is_sticky(tv, u[j] & kIdMask);
+      // positions injected so far: [wb, wb + min(cursor, wlen)) (a batch may end past the window)
+      if (register_each(p, ws, w, tv, c, lane, stk, u[j] & kIdMask, q + 1,
+                        c.wb + min(cursor, c.wlen))) {
+        ok[j] = false;
+        cnt--;
+      }
+    }
+  }
   if (__any_sync(kFull, need && at_end)) {
 #pragma unroll
     for (int j = 0; j < 4; j++) carry_state(p, w, lane, need && at_end && ok[j], u[j] & kIdMask);
   }
-  const bool privatize =
-      PRIV > 0 && __popc(__ballot_sync(kFull, go)) > p.active_threshold;
+  const bool privatize = PRIV > 0 && !tv.sticky &&
+                         __popc(__ballot_sync(kFull, go)) > p.active_threshold;
   if (!privatize) {
     const int pc = (need && !at_end) ? cnt : 0;
     int total;
@@ -536,9 +758,15 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   ws.rbuf = reinterpret_cast<unsigned long long*>(ws.in[1] + window_buf_bytes(W));
   ws.inj = reinterpret_cast<uint32_t*>(ws.rbuf + kReportBuf);
   ws.bar = reinterpret_cast<uint64_t*>(ws.inj + 3 * 32);
+  ws.stk_s = reinterpret_cast<uint32_t*>(ws.bar + 2);
+  ws.stk_q = ws.stk_s + kStickyCap;
+  ws.pend_s = ws.stk_q + kStickyCap;
+  ws.pend_q = ws.pend_s + kPendCap;
+  ws.pend_n = ws.pend_q + kPendCap;
+  if (lane == 0) *ws.pend_n = 0u;
   const int slot = blockIdx.x * kWarpsPerCta + warp;
   WarpRun w;
-  w.top = w.ovf_n = w.ncarry = w.nrep = 0;
+  w.top = w.ovf_n = w.ncarry = w.nrep = w.nstk = 0;
   w.base = 0;
   w.key_hi = 0ull;
   w.ovf = p.ovf + (size_t)slot * p.ovf_cap;
@@ -596,6 +824,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     tv.succ2 = reinterpret_cast<const uint2*>(ib);
     tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
     tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
+    tv.sticky = t->nsticky > 0 ? reinterpret_cast<const uint32_t*>(ib + t->off_sticky) : nullptr;
     tv.cls = ib + t->off_cls;
     tv.t = t;
     tv.pt = s_pt;
@@ -616,6 +845,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       UnitCtx c;
       c.hi = un.hi;
       c.emit_lo = un.emit_lo;
+      w.nstk = 0;  // sticky states are per unit
       w.key_hi = un.key_hi;
       w.base = (uint32_t)un.base;
       int cur = 0;
@@ -661,7 +891,11 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
             const bool rep = ok && is_report(tv, v) && un.lo >= c.emit_lo;
             emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v) | tv.gbits) : 0u,
                         (uint32_t)un.lo);
-            push_entry(p, ws, w, lane, ok && un.lo + 1 < c.hi, v << kEntryPosBits);
+            const bool need = ok && un.lo + 1 < c.hi;
+            bool reg = false;
+            if (tv.sticky)
+              reg = register_each(p, ws, w, tv, c, lane, need && is_sticky(tv, v), v, un.lo, wb);
+            push_entry(p, ws, w, lane, need && !reg, v << kEntryPosBits);
           }
         }
         int cursor = 0;  // next window offset to inject
@@ -683,7 +917,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
             if (cursor < c.wlen) continue;
             break;
           }
-          expand_step<PRIV>(p, ws, w, tv, c, lane, n_expanded);
+          expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
         }
         cur ^= 1;
       }

@@ -244,7 +244,8 @@ void build_image(TileHost& t) {
   t.narrow = t.nstates <= kNarrowMaxStates;
   t.off_cmask = (int32_t)r16(n * (t.narrow ? 8 : 16));
   t.off_rep = t.off_cmask + (int32_t)r16(n * t.cw * 4);
-  t.off_cls = t.off_rep + (int32_t)r16(((n + 31) / 32) * 4);
+  t.off_sticky = t.off_rep + (int32_t)r16(((n + 31) / 32) * 4);
+  t.off_cls = t.off_sticky + (int32_t)r16(((n + 31) / 32) * 4);
   t.image.assign((size_t)t.off_cls + 256, 0);
   if (t.narrow) {  // 4 x u16 per state: 15-bit id, bit 15 = report, 0xffff = none
     uint16_t* s16 = reinterpret_cast<uint16_t*>(t.image.data());
@@ -258,6 +259,7 @@ void build_image(TileHost& t) {
   }
   memcpy(t.image.data() + t.off_cmask, t.cmask.data(), n * t.cw * 4);
   memcpy(t.image.data() + t.off_rep, t.rep.data(), t.rep.size() * 4);
+  memcpy(t.image.data() + t.off_sticky, t.sticky.data(), t.sticky.size() * 4);
   memcpy(t.image.data() + t.off_cls, t.cls.data(), 256);
 }
 
@@ -344,6 +346,20 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
         break;
       }
       base += c.end - c.begin;
+    }
+  }
+  // sticky states: not always-active, a self-loop and every byte accepted; once
+  // such a state matches it matches at every later position of the segment
+  t.sticky.assign((n + 31) / 32, 0);
+  for (int32_t v = 0; v < n; v++) {
+    bool all = true;
+    for (int w = 0; w < 8; w++) all = all && t.bits[(size_t)v * 8 + w] == 0xffffffffu;
+    bool self = false;
+    for (int j = 0; j < 4; j++) self = self || (t.succ[(size_t)v * 4 + j] & 0x7fffffffu) == (uint32_t)v;
+    bool aas = std::find(t.aas.begin(), t.aas.end(), (uint32_t)v) != t.aas.end();
+    if (all && self && !aas) {
+      t.sticky[v >> 5] |= 1u << (v & 31);
+      t.nsticky++;
     }
   }
   build_prefix_tables(t, opts);

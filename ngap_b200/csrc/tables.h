@@ -34,8 +34,10 @@ struct TileHost {
   std::vector<uint32_t> rep;         // ceil(nstates / 32)
   std::vector<uint32_t> sid;         // nstates
   std::vector<uint32_t> aas, start;
-  std::vector<uint8_t> image;        // succ | cmask | rep | cls, 16-byte aligned parts
-  int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
+  std::vector<uint32_t> sticky;      // ceil(nstates / 32): self-loop + every byte, not always-active
+  int32_t nsticky = 0;
+  std::vector<uint8_t> image;        // succ | cmask | rep | sticky | cls, 16-byte aligned parts
+  int32_t off_cmask = 0, off_rep = 0, off_sticky = 0, off_cls = 0;
   PrefixTableHost pt[kMaxDepth];
 };
 
@@ -44,7 +46,7 @@ struct TableOpts {
   int precompute_cutoff = -1;
   int tile_states = 0;              // max states per tile; 0 = fill the image budget
   int64_t max_table_entries = 0;    // 0 = automatic
-  int image_budget = 144 * 1024;    // bytes of shared memory for one tile's image
+  int image_budget = 128 * 1024;    // bytes of shared memory for one tile's image
   int unbounded_tile_states = 256;  // cap for tiles of cyclic CCs (one unit per segment)
   int64_t auto_table_bytes = 12 << 20;  // automatic depth: prefix-table bytes per tile
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
@@ -56,7 +58,7 @@ constexpr int32_t kNarrowMaxStates = 32767;  // 15-bit tile-local ids
 inline int64_t image_bytes(int64_t n, int cw) {
   auto r16 = [](int64_t x) { return (x + 15) & ~(int64_t)15; };
   const int64_t succ = n <= kNarrowMaxStates ? n * 8 : n * 16;
-  return r16(succ) + r16(n * cw * 4) + r16(((n + 31) / 32) * 4) + 256;
+  return r16(succ) + r16(n * cw * 4) + 2 * r16(((n + 31) / 32) * 4) + 256;
 }
 
 // Splits every group into tiles and builds each tile's tables.

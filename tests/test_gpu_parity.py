@@ -99,6 +99,37 @@ def test_deep_prefix_tables(engine, gen, kw, g, depth):
         assert np.array_equal(got, want), algo
 
 
+@pytest.mark.parametrize("window,tile_states", [(0, 0), (64, 0), (0, 6000), (97, 6000)])
+@pytest.mark.parametrize("algo", ["nonblockingpcgroups", "nonblockingallgroups", "blockinggroups"])
+def test_sticky_dotstar(engine, window, tile_states, algo):
+    """`.*` states that are not always active: registered per warp when they
+    first match (with catch-up of injected positions), more than a warp can
+    track with large tiles."""
+    anml, data = W.dotstar_set(seed=21, n_patterns=300, lit_lo=2, lit_hi=4, aas_frac=0.0,
+                               input_len=1 << 16, plant_every=1 << 9, zipf_s=1.6)
+    got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=2, depth=-1,
+                         algorithm=algo, window=window, tile_states=tile_states)
+    assert len(want) > 100
+    assert np.array_equal(got, want)
+
+
+def test_sticky_report_and_start_states(engine):
+    w = W.AnmlWriter()
+    w.ste("a", [ord("x")], ["s"], start="all-input")
+    w.ste("s", None, ["s", "b"], symbol_set="*", report=True)        # reporting .*
+    w.ste("b", [ord("y")], ["c"])
+    w.ste("c", [ord("z")], [], report=True)
+    w.ste("t", None, ["t", "d"], symbol_set="*", start="start-of-data")  # .* from the start
+    w.ste("d", [ord("q")], [], report=True)
+    rng = np.random.default_rng(3)
+    data = rng.choice(np.frombuffer(b"xyzqab", dtype=np.uint8), size=5000)
+    for algo in ("nonblockingpcgroups", "NAPgroups", "blockinggroups"):
+        for window in (0, 50):
+            got, want = run_both(engine, w.text(), data, 4, 1250, group_num=2, depth=2,
+                                 algorithm=algo, window=window)
+            assert np.array_equal(got, want), (algo, window)
+
+
 @pytest.mark.parametrize("chunk,window,tile_states",[(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
 def test_chunking_and_tiling(engine, chunk, window, tile_states):
     """Small chunks, windows and tiles exercise warm-up, carry and tile splits."""
