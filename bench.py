@@ -61,15 +61,18 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(workload):
-    """DRAM bytes per launch of the matching kernel from the committed ncu summary."""
+def profiled_traffic(workload, num_seg):
+    """DRAM bytes (read + write) per launch of the matching kernel, from the
+    committed ncu summary of the same workload and segment count."""
     p = os.path.join(ROOT, "profiles", "match_kernel_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
     v = d.get(workload)
-    return None if v is None else float(v["dram_bytes_per_launch"])
+    if v is None or int(v.get("num_seg", -1)) != num_seg:
+        return None
+    return float(v["dram_bytes_per_launch"])
 
 
 class ClockSampler:
@@ -130,8 +133,19 @@ class ClockSampler:
 
 def algorithmic_bytes(stats, n_in, n_reports, table_bytes):
     """Bytes of the worklist formulation (input + per matched state 24 B of
-    queue/CSR traffic + 8 B per successor tested + 8 B per report + tables)."""
+    queue/CSR traffic + 8 B per successor tested + 8 B per report + tables),
+    from unique-frontier counts (the set of states matched at each position)."""
     return (n_in + stats["matched"] * 24 + stats["matched_deg"] * 8 + n_reports * 8 + table_bytes)
+
+
+def frontier_stats(groups, data, seg_len, nseg=1):
+    """Unique-frontier counts per input byte on the first `nseg` segments
+    (oracle mode 1: bitmap-deduplicated frontier)."""
+    from oracle import oracle
+    n = nseg * seg_len
+    _, st = oracle.match(groups.views(), data[:n], nseg, seg_len, mode=1,
+                         nthreads=os.cpu_count() or 1)
+    return {k: v / n for k, v in st.items()}, n
 
 
 def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
@@ -170,6 +184,8 @@ def main():
     ap.add_argument("--workload", default="hamming_set")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--check", action="store_true", help="verify the reports against the oracle")
+    ap.add_argument("--segments", type=int, default=0,
+                    help="match only the first N segments (smaller case for profiling)")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -222,6 +238,8 @@ def main():
     eng = nb.Engine(local_rank)
     seg_len = cfg["seg_len"]
     num_seg = len(data) // seg_len
+    if args.segments > 0:
+        num_seg = min(num_seg, args.segments)
     n_in = num_seg * seg_len
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -318,17 +336,22 @@ def main():
                 "kernel": "match_kernel", "kernel_ms": mk}
         if not args.no_cpu_baseline:
             cb = cpu_baseline(groups, data[:n_in], seg_len)
-            st = cb.pop("stats")
-            scale = n_in / cb.pop("sample_bytes")
-            cb.pop("sample_reports")
-            stats_full = {k: v * scale for k, v in st.items()}
-            alg = algorithmic_bytes(stats_full, n_in, uniq, tables.device_bytes)
-            roof.update({"achieved": alg / (mk / 1e3) / 1e9, "algorithmic_bytes": alg,
-                         "bytes_per_input_byte": alg / n_in})
-            roof["frac"] = roof["achieved"] / peak
+            for k in ("stats", "sample_bytes", "sample_reports"):
+                cb.pop(k)
             line["cpu_baseline"] = cb
-        tr = profiled_traffic(args.workload)
+        per_byte, sample = frontier_stats(groups, data, seg_len)
+        stats_full = {k: v * n_in for k, v in per_byte.items()}
+        alg = algorithmic_bytes(stats_full, n_in, uniq, tables.device_bytes)
+        roof.update({"achieved": alg / (mk / 1e3) / 1e9, "algorithmic_bytes": alg,
+                     "bytes_per_input_byte": alg / n_in,
+                     "frontier_sample": f"oracle unique frontier over the first {sample} B, "
+                                        f"scaled to {n_in} B"})
+        roof["frac"] = roof["achieved"] / peak
+        tr = profiled_traffic(args.workload, num_seg)
         roof["traffic"] = tr
+        if tr is not None:
+            roof["dram_gbs"] = tr / (mk / 1e3) / 1e9
+            roof["dram_frac"] = roof["dram_gbs"] / peak
         line["roofline"] = roof
         print(json.dumps(line), flush=True)
     if dist is not None:
