@@ -106,7 +106,18 @@ typedef struct ngap_table_opts {
   int precompute_cutoff; /* --precompute-cutoff, -1 = mean list length (precompute_table.cu:171) */
   int tile_states;       /* max states per tile; 0 = automatic */
   int64_t max_table_entries; /* cap on prefix-table list entries per tile; 0 = automatic */
+  int tile_mode;         /* NGAP_TILES_*: where tiles of acyclic CCs keep their tables */
 } ngap_table_opts;
+
+/* Tile modes. Shared: every tile is sized to stage its tables in one CTA's
+ * shared memory (one group per tile). Global: the acyclic CCs of all groups
+ * form few large tiles read through L2, so each input position is looked up
+ * once per large tile instead of once per small one. Auto picks global when
+ * the acyclic CCs need more than two shared-memory tiles. Cyclic CCs always
+ * use shared-memory tiles. No mode changes any report. */
+#define NGAP_TILES_AUTO 0
+#define NGAP_TILES_SHARED 1
+#define NGAP_TILES_GLOBAL 2
 
 /* Replaces GroupCsr/GroupMatchset/GroupNodeAttrs/GroupAAS::init
  * (code/include/commons/group_graph.h:6-109) and ngap::initGroupCsrWithPrec

@@ -51,7 +51,7 @@ class GroupView(ctypes.Structure):
 class TableOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precompute_depth", ctypes.c_int),
                 ("precompute_cutoff", ctypes.c_int), ("tile_states", ctypes.c_int),
-                ("max_table_entries", ctypes.c_int64)]
+                ("max_table_entries", ctypes.c_int64), ("tile_mode", ctypes.c_int)]
 
 
 class MatchParams(ctypes.Structure):

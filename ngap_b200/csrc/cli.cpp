@@ -56,7 +56,7 @@ struct Options {
        try_adaptive_aas = false;
   // additions of this engine
   std::string dump_reports;  // binary dump of the sorted unique reports (u64 each)
-  int window = 0, chunk = 0, tile_states = 0;
+  int window = 0, chunk = 0, tile_states = 0, tile_mode = 0;
 };
 
 bool parse_bool(const std::string& v, bool& out) {
@@ -131,6 +131,7 @@ bool parse_args(int argc, char** argv, Options& o, std::string& err) {
   h["--window"] = i(o.window);
   h["--chunk"] = i(o.chunk);
   h["--tile-states"] = i(o.tile_states);
+  h["--tile-mode"] = i(o.tile_mode);
   for (int k = 1; k < argc; k++) {
     std::string a = argv[k];
     if (a == "-h" || a == "-?" || a == "--help") {
@@ -183,7 +184,8 @@ void print_help() {
                "         --add-aas-interval --active-threshold --precompute-cutoff\n"
                "         --precompute-depth --compress-prec-table --adaptive-aas --tuning\n"
                "         --report-off --validation --quick-validation --max-nfa-size\n"
-               "         --quit-degree --remove-degree --app-name --dump-reports <file>\n";
+               "         --quit-degree --remove-degree --app-name --dump-reports <file>\n"
+               "         --window --chunk --tile-states --tile-mode (0 auto, 1 shared, 2 global)\n";
 }
 
 std::string err_msg() {
@@ -298,6 +300,7 @@ int main(int argc, char** argv) {
   to.precompute_depth = o.precompute_depth;
   to.precompute_cutoff = o.precompute_cutoff;
   to.tile_states = o.tile_states;
+  to.tile_mode = o.tile_mode;
   ngap_tables* tables = nullptr;
   ngap_engine* eng = nullptr;
   if (ngap_tables_build(groups, &to, &tables) != NGAP_OK || ngap_engine_create(0, &eng) != NGAP_OK) {

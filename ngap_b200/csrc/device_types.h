@@ -12,7 +12,8 @@ constexpr int kMaxDepth = 12;        // prefix-memoization depth limit (the refe
 constexpr int kEntryPosBits = 13;    // worklist entry = local_state << 13 | window offset
 constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
 constexpr int kMaxTileStates = 1 << (32 - kEntryPosBits);
-constexpr uint64_t kDenseKeys = 1ull << 18;  // prefix tables with <= 2^18 keys are dense
+constexpr uint64_t kDenseKeys = 1ull << 18;     // prefix tables with <= 2^18 keys are dense
+constexpr uint64_t kMaxDenseKeys = 1ull << 26;  // larger ones are dense when that is smaller
 
 constexpr uint32_t kHashEmpty = 0xffffffffu;
 
@@ -42,9 +43,10 @@ __host__ __device__ inline uint32_t prefix_hash(uint32_t key) {
   return (key * 0x9E3779B1u) ^ (key >> 15);
 }
 
-// A tile: a set of whole CCs of one group, matched by one warp per unit.
-// Its hot tables form one contiguous image, staged into shared memory by the
-// CTA that works on the tile:
+// A tile: a set of whole CCs (of one group, or of several for a global tile),
+// matched by one warp per unit. Its hot tables form one contiguous image,
+// staged into shared memory by the CTA that works on the tile when it fits
+// (global tiles are read in place, through L2):
 //   [succ][cmask: nstates x cw x u32][rep: ceil(nstates/32) x u32][cls: 256 B]
 // succ: up to 4 tile-local successors per state; narrow tiles (< 32767
 // states) store 4 x u16 (bit 15 = report successor, 0xffff = none), wide
@@ -52,7 +54,7 @@ __host__ __device__ inline uint32_t prefix_hash(uint32_t key) {
 // word c/32 = the state accepts byte class c. cls: byte -> class id, live
 // classes first (identity when cw == 8).
 struct TileDev {
-  int32_t group = 0;
+  int32_t group = 0;        // group of the first CC (report ids are in sid)
   int32_t nstates = 0;
   int32_t naas = 0;
   int32_t nstart = 0;
@@ -64,11 +66,12 @@ struct TileDev {
   int32_t narrow = 1;       // 16-bit successors
   int32_t image_bytes = 0;  // multiple of 16
   int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
-  int32_t inj_batch = 32;   // positions injected per worklist refill
+  int32_t inj_batch = 32;   // positions injected per worklist refill (prefix tables)
+  int32_t inj_batch0 = 32;  // the same when the always-active list is scanned
   int32_t nsticky = 0;      // sticky states (bitmap at off_sticky in the image)
   int32_t off_sticky = 0;
   const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
-  const uint32_t* sid = nullptr;    // [nstates] local -> group-local sid
+  const uint32_t* sid = nullptr;    // [nstates] local -> report id (sid | group << 22)
   const uint32_t* aas = nullptr;    // [naas] local ids
   const uint32_t* start = nullptr;  // [nstart] local ids
   PrefixTableDev pt[kMaxDepth];

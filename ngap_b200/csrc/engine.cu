@@ -171,6 +171,10 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     set_error("precompute_depth must be in -1..%d (got %d)", kMaxDepth, o.precompute_depth);
     return NGAP_E_INVALID;
   }
+  if (o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
+    set_error("tile_mode must be NGAP_TILES_AUTO, _SHARED or _GLOBAL (got %d)", o.tile_mode);
+    return NGAP_E_INVALID;
+  }
   std::unique_ptr<ngap_tables> t(new ngap_tables());
   t->device = o.device;
   CUDA_TRY(cudaSetDevice(o.device));
@@ -179,6 +183,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
   to.precompute_cutoff = o.precompute_cutoff;
   to.tile_states = o.tile_states;
   to.max_table_entries = o.max_table_entries;
+  to.tile_mode = o.tile_mode;
   int rc = build_tiles(g->gs, to, t->tiles);
   if (rc != NGAP_OK) return rc;
   t->num_groups = (int)g->gs.groups.size();
@@ -205,6 +210,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.off_rep = th.off_rep;
     d.off_cls = th.off_cls;
     d.inj_batch = th.inj_batch;
+    d.inj_batch0 = th.inj_batch0;
     d.nsticky = th.nsticky;
     d.off_sticky = th.off_sticky;
     if ((rc = t->upload(th.image, &d.image)) != NGAP_OK) return rc;

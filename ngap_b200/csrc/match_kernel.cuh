@@ -130,7 +130,6 @@ struct TileView {
   int cw;
   int narrow;
   uint32_t nlive;  // live classes: base of the prefix-table keys
-  uint32_t gbits;
 };
 
 // Successors of v in the 32-bit convention (bit 31 = report, kNoSucc = none).
@@ -337,7 +336,7 @@ __device__ __forceinline__ void report4(const MatchParams& p, WarpSmem& ws, Warp
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const bool rep = in_range && ok[j] && (u[j] >> 31);
-    emit_report(p, ws, w, lane, rep, rep ? (__ldg(tv.t->sid + (u[j] & kIdMask)) | tv.gbits) : 0u,
+    emit_report(p, ws, w, lane, rep, rep ? (__ldg(tv.t->sid + (u[j] & kIdMask))) : 0u,
                 (uint32_t)q);
   }
 }
@@ -365,7 +364,7 @@ __device__ __forceinline__ void sticky_at(const MatchParams& p, WarpSmem& ws, Wa
   const int r = (int)(t - c.wb);
   const uint32_t sym = act ? c.in[r] : 0u;
   const bool rs = act && srep && t >= c.emit_lo;
-  emit_report(p, ws, w, lane, rs, rs ? (__ldg(tv.t->sid + s) | tv.gbits) : 0u, (uint32_t)t);
+  emit_report(p, ws, w, lane, rs, rs ? __ldg(tv.t->sid + s) : 0u, (uint32_t)t);
   bool ok[4];
 #pragma unroll
   for (int j = 0; j < 4; j++)
@@ -456,7 +455,7 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
       const uint32_t a = __ldg(t.aas + i);
       const bool ok = valid && accepts(tv, a, s);
       const bool rep = ok && is_report(tv, a) && q >= c.emit_lo;
-      emit_report(p, ws, w, lane, rep, rep ? (__ldg(t.sid + a) | tv.gbits) : 0u, (uint32_t)q);
+      emit_report(p, ws, w, lane, rep, rep ? (__ldg(t.sid + a)) : 0u, (uint32_t)q);
       push_entry(p, ws, w, lane, ok && q + 1 < c.hi, (a << kEntryPosBits) | (uint32_t)r);
       n_injected += ok;
     }
@@ -489,7 +488,7 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
       for (int i = 0; i < mx; i++) {
         const bool ok = i < len && q + d >= c.emit_lo;
         const uint32_t v = ok ? __ldg(pt.rlist + rb + i) : 0u;
-        emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v) | tv.gbits) : 0u, (uint32_t)(q + d));
+        emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v)) : 0u, (uint32_t)(q + d));
       }
     }
   }
@@ -586,7 +585,7 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
       const uint32_t s = ws.stk_s[i];
       const bool act = valid && t > (int64_t)ws.stk_q[i];
       const bool rs = act && is_report(tv, s) && t >= c.emit_lo;
-      emit_report(p, ws, w, lane, rs, rs ? (__ldg(tv.t->sid + s) | tv.gbits) : 0u, (uint32_t)t);
+      emit_report(p, ws, w, lane, rs, rs ? __ldg(tv.t->sid + s) : 0u, (uint32_t)t);
       const uint4 sc = load_succ(tv, s);
       const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
       bool ok[4];
@@ -747,6 +746,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   __shared__ int s_task;
   __shared__ unsigned s_next;
   __shared__ __align__(16) PrefixTableDev s_pt[kMaxDepth];
+  __shared__ __align__(16) uint8_t s_cls[256];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = p.window;
   uint8_t* image = smem_raw;
@@ -811,10 +811,13 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       for (int i = threadIdx.x; i < t->image_bytes / 16; i += kCtaThreads) dst[i] = __ldg(src + i);
       staged = tk.tile;
     }
-    {  // the tile's prefix-table descriptors, read at every injection
+    {  // the tile's prefix-table descriptors, read at every injection, and its byte classes
       const uint32_t* src = reinterpret_cast<const uint32_t*>(t->pt);
       uint32_t* dst = reinterpret_cast<uint32_t*>(s_pt);
       for (int i = threadIdx.x; i < (int)(sizeof(s_pt) / 4); i += kCtaThreads) dst[i] = src[i];
+      if (threadIdx.x < 64)
+        reinterpret_cast<uint32_t*>(s_cls)[threadIdx.x] =
+            __ldg(reinterpret_cast<const uint32_t*>(t->image + t->off_cls) + threadIdx.x);
     }
     if (threadIdx.x == 0) s_next = (unsigned)tk.ubegin;
     __syncthreads();
@@ -825,15 +828,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
     tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
     tv.sticky = t->nsticky > 0 ? reinterpret_cast<const uint32_t*>(ib + t->off_sticky) : nullptr;
-    tv.cls = ib + t->off_cls;
+    tv.cls = s_cls;
     tv.t = t;
     tv.pt = s_pt;
     tv.cw = t->cw;
     tv.narrow = t->narrow;
     tv.nlive = (uint32_t)t->nlive;
-    tv.gbits = (uint32_t)t->group << 22;
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
-    const int batch = depth == 0 ? 32 : t->inj_batch;
+    const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
     const bool translate = t->cw != 8;
 
     while (!dead) {
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
             const uint32_t v = i < t->nstart ? __ldg(t->start + i) : 0u;
             const bool ok = i < t->nstart && accepts(tv, v, s0);
             const bool rep = ok && is_report(tv, v) && un.lo >= c.emit_lo;
-            emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v) | tv.gbits) : 0u,
+            emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v)) : 0u,
                         (uint32_t)un.lo);
             const bool need = ok && un.lo + 1 < c.hi;
             bool reg = false;
@@ -900,7 +902,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         }
         int cursor = 0;  // next window offset to inject
         while (true) {
-          if (w.top < kInjectLow && cursor < c.wlen) {
+          // inject only when the overflow stack is empty, so that it holds at
+          // most one batch's excess
+          if (w.top < kInjectLow && w.ovf_n == 0 && cursor < c.wlen) {
             inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
             cursor += batch;
             continue;

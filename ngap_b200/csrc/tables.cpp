@@ -1,9 +1,10 @@
 // Tiles, byte classes, shared-memory images and prefix-memoization tables.
 //
-// A tile is a set of whole CCs of one group. CCs never share states or edges,
-// so splitting a group into tiles changes no report: a report keeps its
-// group-local sid (TileHost::sid) and its group index. Two facts about the
-// graph are used:
+// A tile is a set of whole CCs: of one group for shared-memory tiles, of any
+// groups for global tiles. CCs never share states or edges, so the way CCs
+// are packed into tiles changes no report: every state keeps its report id
+// (group-local sid | group << 22, TileHost::sid). Two facts about the graph
+// are used:
 //   * an edge into an always-active state is redundant, because the reference
 //     puts every always-active state in every frontier (code/src/ngap/ngap.cu:
 //     2252-2256); such edges are dropped here;
@@ -28,15 +29,20 @@
 #include "tables.h"
 
 #include <algorithm>
+#include <array>
+#include <atomic>
 #include <cstring>
 #include <map>
+#include <numeric>
+#include <thread>
 
 namespace ngap {
 
 namespace {
 
 struct CcInfo {
-  int32_t begin, end;
+  int32_t group;        // group index (report ids carry it in bits 22 and up)
+  int32_t begin, end;   // group-local state range
   bool bounded;
   int32_t max_path;
 };
@@ -99,143 +105,187 @@ inline bool accepts_cls(const TileHost& t, uint32_t v, int c) {
 
 inline bool is_report(const TileHost& t, uint32_t v) { return (t.rep[v >> 5] >> (v & 31)) & 1u; }
 
-// Lays out one table; false when a list is too long for the hashed slot format.
-bool finish_table(PrefixTableHost& pt, uint64_t space,
-                  const std::map<uint32_t, std::vector<uint32_t>>& lists, const TileHost& t,
+// One level of prefix lists: the non-empty keys in ascending order with their
+// state lists (sorted, deduplicated), flat.
+struct Level {
+  std::vector<uint32_t> keys;
+  std::vector<uint32_t> off{0};  // keys.size() + 1
+  std::vector<uint32_t> list;
+};
+
+// Lays out one table, dense (offsets indexed by key) or hashed, whichever
+// takes fewer bytes; false when a list is too long for the hashed slot format.
+bool finish_table(PrefixTableHost& pt, uint64_t space, const Level& lv, const TileHost& t,
                   int cutoff_opt) {
   pt = PrefixTableHost();
-  pt.dense = space <= kDenseKeys;
-  int64_t total = 0, nonzero = 0;
+  const size_t nz = lv.keys.size();
+  bool any_rep = false;
+  for (uint32_t v : lv.list) any_rep = any_rep || is_report(t, v);
+  uint64_t cap = 16;
+  while (cap < 2 * (uint64_t)nz) cap <<= 1;
+  const uint64_t dense_bytes = (space + 1) * 4 * (any_rep ? 2 : 1);
+  pt.dense = space <= kDenseKeys || (space <= kMaxDenseKeys && dense_bytes <= cap * 16);
+  pt.vlist = lv.list;
   if (pt.dense) {
     pt.voff.assign(space + 1, 0);
-    pt.roff.assign(space + 1, 0);
-    std::vector<uint32_t> vcount(space, 0), rcount(space, 0);
-    for (auto& kv : lists) {
-      vcount[kv.first] = (uint32_t)kv.second.size();
-      for (uint32_t v : kv.second)
-        if (is_report(t, v)) rcount[kv.first]++;
+    if (any_rep) pt.roff.assign(space + 1, 0);
+    for (size_t i = 0; i < nz; i++) {
+      pt.voff[lv.keys[i] + 1] = lv.off[i + 1] - lv.off[i];
+      if (any_rep) {
+        uint32_t r = 0;
+        for (uint32_t j = lv.off[i]; j < lv.off[i + 1]; j++) r += is_report(t, lv.list[j]) ? 1u : 0u;
+        pt.roff[lv.keys[i] + 1] = r;
+      }
     }
     for (uint64_t k = 0; k < space; k++) {
-      pt.voff[k + 1] = pt.voff[k] + vcount[k];
-      pt.roff[k + 1] = pt.roff[k] + rcount[k];
+      pt.voff[k + 1] += pt.voff[k];
+      if (any_rep) pt.roff[k + 1] += pt.roff[k];
     }
-    pt.vlist.resize(pt.voff[space]);
-    pt.rlist.resize(pt.roff[space]);
-    for (auto& kv : lists) {
-      uint32_t vo = pt.voff[kv.first], ro = pt.roff[kv.first];
-      for (uint32_t v : kv.second) {
-        pt.vlist[vo++] = v;
-        if (is_report(t, v)) pt.rlist[ro++] = v;
-      }
-    }
+    for (uint32_t v : lv.list)
+      if (is_report(t, v)) pt.rlist.push_back(v);
   } else {
-    uint64_t cap = 16;
-    while (cap < 2 * lists.size()) cap <<= 1;
     pt.hmask = (uint32_t)(cap - 1);
     pt.slots.assign(cap * 4, 0);
-    for (uint64_t s = 0; s < cap; s++) pt.slots[s * 4] = kHashEmpty;
-    for (auto& kv : lists) {
-      const uint32_t vb = (uint32_t)pt.vlist.size(), rb = (uint32_t)pt.rlist.size();
-      for (uint32_t v : kv.second) {
-        pt.vlist.push_back(v);
-        if (is_report(t, v)) pt.rlist.push_back(v);
-      }
-      const uint32_t vl = (uint32_t)pt.vlist.size() - vb, rl = (uint32_t)pt.rlist.size() - rb;
+    for (uint64_t sl = 0; sl < cap; sl++) pt.slots[sl * 4] = kHashEmpty;
+    for (size_t i = 0; i < nz; i++) {
+      const uint32_t vb = lv.off[i], rb = (uint32_t)pt.rlist.size();
+      for (uint32_t j = lv.off[i]; j < lv.off[i + 1]; j++)
+        if (is_report(t, lv.list[j])) pt.rlist.push_back(lv.list[j]);
+      const uint32_t vl = lv.off[i + 1] - vb, rl = (uint32_t)pt.rlist.size() - rb;
       if (vl >= 65536 || rl >= 65536) return false;
-      uint32_t h = prefix_hash(kv.first) & pt.hmask;
+      uint32_t h = prefix_hash(lv.keys[i]) & pt.hmask;
       while (pt.slots[(size_t)h * 4] != kHashEmpty) h = (h + 1) & pt.hmask;
-      uint32_t* sl = &pt.slots[(size_t)h * 4];
-      sl[0] = kv.first;
-      sl[1] = vb;
-      sl[2] = rb;
-      sl[3] = (vl << 16) | rl;
+      uint32_t* e = &pt.slots[(size_t)h * 4];
+      e[0] = lv.keys[i];
+      e[1] = vb;
+      e[2] = rb;
+      e[3] = (vl << 16) | rl;
     }
   }
-  if (pt.rlist.empty()) pt.roff.clear();  // no reports: the offsets are never read
-  for (auto& kv : lists) {
-    total += (int64_t)kv.second.size();
-    nonzero++;
-  }
   // PrecTable::calcCutoff (precompute_table.cu:171-186): mean non-empty list length.
-  pt.cutoff = nonzero > 0 ? (int32_t)(total / nonzero) : 0;
+  pt.cutoff = nz > 0 ? (int32_t)(lv.list.size() / nz) : 0;
   if (cutoff_opt >= 0) pt.cutoff = cutoff_opt;
   return true;
 }
 
-void build_prefix_tables(TileHost& t, const TableOpts& opts) {
-  // depth < 0: as deep as the size caps allow
-  const int want = opts.precompute_depth < 0 ? kMaxDepth
-                                             : std::max(1, std::min(opts.precompute_depth, kMaxDepth));
-  const int64_t cap = opts.max_table_entries > 0 ? opts.max_table_entries : (int64_t)2 << 20;
-  // keys are base-L numbers over the L live classes (the dead class ends paths)
-  const uint32_t L = (uint32_t)t.nlive;
-  std::map<uint32_t, std::vector<uint32_t>> prev, cur;
-  for (uint32_t c = 0; c < L; c++) {
-    std::vector<uint32_t> l;
-    for (uint32_t a : t.aas)
-      if (accepts_cls(t, a, (int)c)) l.push_back(a);
-    if (!l.empty()) prev[c] = std::move(l);
-  }
-  finish_table(t.pt[0], (uint64_t)L, prev, t, opts.precompute_cutoff);
-  uint64_t space = (uint64_t)L;
-  t.depth = 1;
-  std::vector<uint32_t> mark(t.nstates, 0);
-  uint32_t stamp = 0;
-  for (int d = 2; d <= want; d++) {
-    if (space * (uint64_t)L >= (1ull << 32)) break;  // keys are 32-bit
-    space *= (uint64_t)L;
-    cur.clear();
-    int64_t total = 0;
-    bool too_big = false;
-    for (auto& kv : prev) {
-      for (int c = 0; c < (int)L && !too_big; c++) {
-        std::vector<uint32_t> l;
+// Level d from level d - 1: key * L + c -> successors of key's states that
+// accept class c. Keys stay ascending because each slice of `prev` is expanded
+// in order. Work is split over threads by slices of prev's keys; false when
+// more than `cap` entries would be produced.
+bool next_level(const Level& prev, const TileHost& t, uint32_t L, int64_t cap, Level& cur) {
+  const size_t nk = prev.keys.size();
+  int nth = (int)std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+  nth = (int)std::min<size_t>(nth, nk / 256 + 1);
+  std::vector<Level> part(nth);
+  std::atomic<int64_t> total{0};
+  auto work = [&](int id) {
+    const size_t lo = nk * id / nth, hi = nk * (id + 1) / nth;
+    Level& out = part[id];
+    std::vector<uint32_t> mark(t.nstates, 0), l;
+    uint32_t stamp = 0;
+    int64_t reported = 0;
+    for (size_t i = lo; i < hi; i++) {
+      for (uint32_t c = 0; c < L; c++) {
+        l.clear();
         stamp++;
-        for (uint32_t v : kv.second) {
-          const uint32_t* sc = &t.succ[(size_t)v * 4];
-          for (int j = 0; j < 4; j++) {
-            uint32_t u = sc[j];
+        for (uint32_t j = prev.off[i]; j < prev.off[i + 1]; j++) {
+          const uint32_t* sc = &t.succ[(size_t)prev.list[j] * 4];
+          for (int k = 0; k < 4; k++) {
+            uint32_t u = sc[k];
             if (u == kNoSucc) continue;
             u &= 0x7fffffffu;
-            if (!accepts_cls(t, u, c) || mark[u] == stamp) continue;
+            if (mark[u] == stamp || !accepts_cls(t, u, (int)c)) continue;
             mark[u] = stamp;
             l.push_back(u);
           }
         }
-        if (!l.empty()) {
-          std::sort(l.begin(), l.end());
-          total += (int64_t)l.size();
-          cur[kv.first * L + (uint32_t)c] = std::move(l);
-          if (total > cap) too_big = true;
-        }
+        if (l.empty()) continue;
+        std::sort(l.begin(), l.end());
+        out.keys.push_back(prev.keys[i] * L + c);
+        out.list.insert(out.list.end(), l.begin(), l.end());
+        out.off.push_back((uint32_t)out.list.size());
       }
-      if (too_big) break;
+      if ((i & 255) == 255) {  // publish progress; stop once all threads together pass cap
+        const int64_t now = (int64_t)out.list.size();
+        if (total.fetch_add(now - reported) + (now - reported) > cap) return;
+        reported = now;
+      }
     }
-    if (too_big) break;
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < nth; i++) th.emplace_back(work, i);
+  work(0);
+  for (auto& x : th) x.join();
+  int64_t sum = 0;
+  for (auto& pp : part) sum += (int64_t)pp.list.size();
+  if (sum > cap || sum >= (int64_t)UINT32_MAX) return false;
+  cur = Level();
+  cur.keys.reserve(std::accumulate(part.begin(), part.end(), (size_t)0,
+                                   [](size_t a, const Level& x) { return a + x.keys.size(); }));
+  cur.list.reserve((size_t)sum);
+  for (auto& pp : part) {
+    const uint32_t base = (uint32_t)cur.list.size();
+    cur.keys.insert(cur.keys.end(), pp.keys.begin(), pp.keys.end());
+    for (size_t i = 1; i < pp.off.size(); i++) cur.off.push_back(base + pp.off[i]);
+    cur.list.insert(cur.list.end(), pp.list.begin(), pp.list.end());
+  }
+  return true;
+}
+
+int64_t table_bytes(const PrefixTableHost& pk) {
+  return 4 * (int64_t)(pk.voff.size() + pk.roff.size() + pk.slots.size() + pk.vlist.size() +
+                       pk.rlist.size());
+}
+
+void build_prefix_tables(TileHost& t, const TableOpts& opts, bool global) {
+  // depth < 0: as deep as the size caps allow
+  const int want = opts.precompute_depth < 0 ? kMaxDepth
+                                             : std::max(1, std::min(opts.precompute_depth, kMaxDepth));
+  const int64_t cap = opts.max_table_entries > 0
+                          ? opts.max_table_entries
+                          : (global ? opts.global_table_entries : (int64_t)2 << 20);
+  const int64_t budget = global ? opts.auto_global_table_bytes : opts.auto_table_bytes;
+  // keys are base-L numbers over the L live classes (the dead class ends paths)
+  const uint32_t L = (uint32_t)t.nlive;
+  Level prev;
+  for (uint32_t c = 0; c < L; c++) {
+    const size_t before = prev.list.size();
+    for (uint32_t a : t.aas)
+      if (accepts_cls(t, a, (int)c)) prev.list.push_back(a);
+    if (prev.list.size() == before) continue;
+    prev.keys.push_back(c);
+    prev.off.push_back((uint32_t)prev.list.size());
+  }
+  finish_table(t.pt[0], (uint64_t)L, prev, t, opts.precompute_cutoff);
+  uint64_t space = (uint64_t)L;
+  int64_t bytes = table_bytes(t.pt[0]);
+  t.depth = 1;
+  for (int d = 2; d <= want; d++) {
+    if (space * (uint64_t)L >= (1ull << 32)) break;  // keys are 32-bit
+    space *= (uint64_t)L;
+    Level cur;
+    if (!next_level(prev, t, L, cap, cur)) break;
     if (!finish_table(t.pt[d - 1], space, cur, t, opts.precompute_cutoff)) {
       t.pt[d - 1] = PrefixTableHost();
       break;
     }
-    if (opts.precompute_depth < 0) {  // automatic depth: bounded device bytes per tile
-      int64_t bytes = 0;
-      for (int k = 0; k < d; k++) {
-        const PrefixTableHost& pk = t.pt[k];
-        bytes += 4 * (int64_t)(pk.voff.size() + pk.roff.size() + pk.slots.size() +
-                               pk.vlist.size() + pk.rlist.size());
-      }
-      if (bytes > opts.auto_table_bytes) {
-        t.pt[d - 1] = PrefixTableHost();
-        break;
-      }
+    bytes += table_bytes(t.pt[d - 1]);
+    if (opts.precompute_depth < 0 && bytes > budget) {  // automatic depth: bounded device bytes
+      t.pt[d - 1] = PrefixTableHost();
+      break;
     }
     t.depth = d;
-    prev.swap(cur);
+    prev.keys.swap(cur.keys);
+    prev.off.swap(cur.off);
+    prev.list.swap(cur.list);
   }
   // positions injected per refill: keep one refill's lists within about half
   // of a warp's shared worklist
   const PrefixTableHost& deep = t.pt[t.depth - 1];
   const int mean = std::max(1, deep.cutoff);
   t.inj_batch = std::max(1, std::min(32, 512 / (mean + 1)));
+  // scanning the always-active list: table 1's mean is the states matched per position
+  t.inj_batch0 = std::max(1, std::min(32, 2048 / (std::max(1, t.pt[0].cutoff) + 1)));
 }
 
 void build_image(TileHost& t) {
@@ -268,16 +318,17 @@ int degree_error() {
   return NGAP_E_INVALID;
 }
 
-bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, const TableOpts& opts,
-               std::vector<TileHost>& tiles) {
+bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
+               const TableOpts& opts, std::vector<TileHost>& tiles) {
   if (ccs.empty()) return true;
   TileHost t;
-  t.group = gi;
+  t.group = ccs[0].group;
   int32_t n = 0;
   bool bounded = true;
   int32_t mp = 0;
   Partition part;
   for (auto& c : ccs) {
+    const GroupGraph& g = gs.groups[c.group];
     n += c.end - c.begin;
     bounded = bounded && c.bounded;
     mp = std::max(mp, c.max_path);
@@ -286,6 +337,7 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   t.nstates = n;
   t.num_ccs = (int32_t)ccs.size();
   t.max_path = bounded ? mp : -1;
+  t.global = global;
   t.cw = class_words(part.n);
   t.cls.resize(256);
   if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
@@ -295,9 +347,11 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   } else {
     // bytes no state accepts share one (dead) class; number it last
     uint32_t any[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (auto& c : ccs)
+    for (auto& c : ccs) {
+      const GroupGraph& g = gs.groups[c.group];
       for (int32_t v = c.begin; v < c.end; v++)
         for (int w = 0; w < 8; w++) any[w] |= g.bits[(size_t)v * 8 + w];
+    }
     int dead = -1;
     for (int b = 0; b < 256 && dead < 0; b++)
       if (!((any[b >> 5] >> (b & 31)) & 1u)) dead = part.id[b];
@@ -314,10 +368,13 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
   t.cmask.assign((size_t)n * t.cw, 0);
   t.rep.assign((n + 31) / 32, 0);
   t.sid.resize(n);
+  std::vector<uint32_t> aas_bit((n + 31) / 32, 0);
   int32_t local = 0;
   for (auto& c : ccs) {
+    const GroupGraph& g = gs.groups[c.group];
+    const int32_t first = local;  // local id of the CC's first state
     for (int32_t v = c.begin; v < c.end; v++, local++) {
-      t.sid[local] = (uint32_t)v;
+      t.sid[local] = (uint32_t)v | ((uint32_t)c.group << 22);
       const uint32_t* bv = &g.bits[(size_t)v * 8];
       for (int w = 0; w < 8; w++) t.bits[(size_t)local * 8 + w] = bv[w];
       for (int b = 0; b < 256; b++)
@@ -326,27 +383,23 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
           t.cmask[(size_t)local * t.cw + (cl >> 5)] |= 1u << (cl & 31);
         }
       if (g.attrs[v] & 2) t.rep[local >> 5] |= 1u << (local & 31);
-      if (g.attrs[v] & 1) t.aas.push_back((uint32_t)local);
+      if (g.attrs[v] & 1) {
+        t.aas.push_back((uint32_t)local);
+        aas_bit[local >> 5] |= 1u << (local & 31);
+      }
       int j = 0;
       for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
         int32_t u = g.cols[k];
         if (g.attrs[u] & 1) continue;  // redundant: u is active at every position
         if (j >= 4) return false;      // the degree limiter guarantees at most 4
-        uint32_t ul = (uint32_t)(u - c.begin + (local - (v - c.begin)));
+        uint32_t ul = (uint32_t)(first + (u - c.begin));
         t.succ[(size_t)local * 4 + j++] = ul | ((g.attrs[u] & 2) ? 0x80000000u : 0u);
       }
     }
-  }
-  // start-of-data states in ascending sid order
-  for (int32_t s : g.starts) {
-    int32_t base = 0;
-    for (auto& c : ccs) {
-      if (s >= c.begin && s < c.end) {
-        t.start.push_back((uint32_t)(base + s - c.begin));
-        break;
-      }
-      base += c.end - c.begin;
-    }
+    // start-of-data states of the CC, ascending (the group's list is ascending)
+    auto lo = std::lower_bound(g.starts.begin(), g.starts.end(), c.begin);
+    for (auto it = lo; it != g.starts.end() && *it < c.end; ++it)
+      t.start.push_back((uint32_t)(first + (*it - c.begin)));
   }
   // sticky states: not always-active, a self-loop and every byte accepted; once
   // such a state matches it matches at every later position of the segment
@@ -356,61 +409,137 @@ bool emit_tile(const GroupGraph& g, int gi, const std::vector<CcInfo>& ccs, cons
     for (int w = 0; w < 8; w++) all = all && t.bits[(size_t)v * 8 + w] == 0xffffffffu;
     bool self = false;
     for (int j = 0; j < 4; j++) self = self || (t.succ[(size_t)v * 4 + j] & 0x7fffffffu) == (uint32_t)v;
-    bool aas = std::find(t.aas.begin(), t.aas.end(), (uint32_t)v) != t.aas.end();
+    const bool aas = (aas_bit[v >> 5] >> (v & 31)) & 1u;
     if (all && self && !aas) {
       t.sticky[v >> 5] |= 1u << (v & 31);
       t.nsticky++;
     }
   }
-  build_prefix_tables(t, opts);
+  build_prefix_tables(t, opts, global);
   build_image(t);
   tiles.push_back(std::move(t));
   return true;
 }
 
+// Packs CCs into tiles in order: a tile is closed when the next CC would pass
+// `max_states` or, for shared-memory tiles, the image budget.
+class TilePacker {
+ public:
+  TilePacker(const GroupSet& gs, const TableOpts& opts, bool global, int64_t max_states,
+             std::vector<TileHost>& tiles)
+      : gs_(gs), opts_(opts), global_(global), max_states_(max_states), tiles_(tiles) {}
+
+  bool add(const CcInfo& ci) {
+    const GroupGraph& g = gs_.groups[ci.group];
+    const int32_t sz = ci.end - ci.begin;
+    Partition trial = part_;
+    if (!global_)
+      for (int32_t v = ci.begin; v < ci.end; v++) trial.refine(&g.bits[(size_t)v * 8]);
+    const bool fits = n_ + sz <= max_states_ &&
+                      (global_ || image_bytes(n_ + sz, class_words(trial.n)) <= opts_.image_budget);
+    if (!open_.empty() && !fits) {
+      if (!flush()) return false;
+      if (!global_)
+        for (int32_t v = ci.begin; v < ci.end; v++) part_.refine(&g.bits[(size_t)v * 8]);
+    } else {
+      part_ = trial;
+    }
+    open_.push_back(ci);
+    n_ += sz;
+    return true;
+  }
+
+  bool flush() {
+    const bool ok = emit_tile(gs_, open_, global_, opts_, tiles_);
+    open_.clear();
+    n_ = 0;
+    part_ = Partition();
+    return ok;
+  }
+
+ private:
+  const GroupSet& gs_;
+  const TableOpts& opts_;
+  bool global_;
+  int64_t max_states_;
+  std::vector<TileHost>& tiles_;
+  std::vector<CcInfo> open_;
+  int64_t n_ = 0;
+  Partition part_;
+};
+
 }  // namespace
 
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles) {
   tiles.clear();
-  // Acyclic tiles get parallelism from chunks, so they fill the image budget.
-  // A cyclic tile is one sequential unit per segment, so those stay small to
-  // give the GPU enough independent units.
-  const int64_t max_states[2] = {
-      opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2,
-      opts.tile_states > 0 ? opts.tile_states : (int64_t)opts.unbounded_tile_states};
+  std::vector<CcInfo> ccs;
+  // acyclic CCs clustered by alphabet (the bytes any of their states accepts)
+  std::map<std::array<uint32_t, 8>, std::vector<int>> clusters;
   for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
     const GroupGraph& g = gs.groups[gi];
-    std::vector<CcInfo> open[2];  // [0] bounded, [1] unbounded
-    int32_t open_n[2] = {0, 0};
-    Partition open_part[2];
     const int nccs = (int)g.cc_begin.size() - 1;
     for (int c = 0; c < nccs; c++) {
       CcInfo ci;
+      ci.group = gi;
       ci.begin = g.cc_begin[c];
       ci.end = g.cc_begin[c + 1];
       int32_t lp = cc_longest_path(g, ci.begin, ci.end);
       ci.bounded = lp >= 0 && lp <= opts.max_warmup;
       ci.max_path = ci.bounded ? lp : -1;
-      const int k = ci.bounded ? 0 : 1;
-      const int32_t sz = ci.end - ci.begin;
-      Partition trial = open_part[k];
-      for (int32_t v = ci.begin; v < ci.end; v++) trial.refine(&g.bits[(size_t)v * 8]);
-      const bool fits = open_n[k] + sz <= max_states[k] &&
-                        image_bytes(open_n[k] + sz, class_words(trial.n)) <= opts.image_budget;
-      if (!open[k].empty() && !fits) {
-        if (!emit_tile(g, gi, open[k], opts, tiles)) return degree_error();
-        open[k].clear();
-        open_n[k] = 0;
-        open_part[k] = Partition();
-        for (int32_t v = ci.begin; v < ci.end; v++) open_part[k].refine(&g.bits[(size_t)v * 8]);
-      } else {
-        open_part[k] = trial;
+      if (ci.bounded) {
+        std::array<uint32_t, 8> alpha{};
+        for (int32_t v = ci.begin; v < ci.end; v++)
+          for (int w = 0; w < 8; w++) alpha[w] |= g.bits[(size_t)v * 8 + w];
+        clusters[alpha].push_back((int)ccs.size());
       }
-      open[k].push_back(ci);
-      open_n[k] += sz;
+      ccs.push_back(ci);
     }
-    for (int k = 0; k < 2; k++)
-      if (!emit_tile(g, gi, open[k], opts, tiles)) return degree_error();
+  }
+  // A cluster of acyclic CCs becomes global tiles when it would need more than
+  // two shared-memory tiles and its bytes fall into at most 32 classes (keys of
+  // deep prefix tables stay small); everything else, cyclic CCs included, uses
+  // shared-memory tiles. NGAP_TILES_GLOBAL takes every acyclic CC global.
+  std::vector<char> in_global(ccs.size(), 0);
+  std::vector<std::vector<int>> global_sets;
+  if (opts.tile_mode == 2) {
+    global_sets.emplace_back();
+    for (size_t i = 0; i < ccs.size(); i++)
+      if (ccs[i].bounded) global_sets.back().push_back((int)i);
+  } else if (opts.tile_mode == 0) {
+    for (auto& kv : clusters) {
+      Partition part;
+      int64_t n = 0;
+      for (int i : kv.second) {
+        const GroupGraph& g = gs.groups[ccs[i].group];
+        n += ccs[i].end - ccs[i].begin;
+        for (int32_t v = ccs[i].begin; v < ccs[i].end; v++) part.refine(&g.bits[(size_t)v * 8]);
+      }
+      if (class_words(part.n) == 1 && image_bytes(n, 1) > 2 * (int64_t)opts.image_budget)
+        global_sets.push_back(kv.second);
+    }
+  }
+  // Acyclic tiles get parallelism from chunks, so they fill the budget. A
+  // cyclic tile is one sequential unit per segment, so those stay small to
+  // give the GPU enough independent units.
+  const int64_t cap_bounded = opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2;
+  const int64_t cap_cyclic = opts.tile_states > 0 ? opts.tile_states : (int64_t)opts.unbounded_tile_states;
+  for (auto& set : global_sets) {
+    std::sort(set.begin(), set.end());  // (group, CC) order
+    TilePacker pk(gs, opts, true, cap_bounded, tiles);
+    for (int i : set) {
+      in_global[i] = 1;
+      if (!pk.add(ccs[i])) return degree_error();
+    }
+    if (!pk.flush()) return degree_error();
+  }
+  for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
+    TilePacker b(gs, opts, false, cap_bounded, tiles), u(gs, opts, false, cap_cyclic, tiles);
+    for (size_t i = 0; i < ccs.size(); i++) {
+      const CcInfo& ci = ccs[i];
+      if (ci.group != gi || in_global[i]) continue;
+      if (!(ci.bounded ? b : u).add(ci)) return degree_error();
+    }
+    if (!b.flush() || !u.flush()) return degree_error();
   }
   return NGAP_OK;
 }

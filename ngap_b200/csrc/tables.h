@@ -27,12 +27,14 @@ struct TileHost {
   int32_t ncls = 0, cw = 8, nlive = 0;
   bool narrow = true;                // 16-bit successor ids in the image
   int32_t inj_batch = 32;            // positions injected per worklist refill
+  int32_t inj_batch0 = 32;           // the same without prefix tables (AAS scan)
+  bool global = false;               // tables read through L2, never staged in shared memory
   std::vector<uint8_t> cls;          // 256: byte -> class, live classes first
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
   std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
   std::vector<uint32_t> cmask;       // nstates * cw
   std::vector<uint32_t> rep;         // ceil(nstates / 32)
-  std::vector<uint32_t> sid;         // nstates
+  std::vector<uint32_t> sid;         // nstates: report id, group-local sid | group << 22
   std::vector<uint32_t> aas, start;
   std::vector<uint32_t> sticky;      // ceil(nstates / 32): self-loop + every byte, not always-active
   int32_t nsticky = 0;
@@ -50,6 +52,9 @@ struct TableOpts {
   int unbounded_tile_states = 256;  // cap for tiles of cyclic CCs (one unit per segment)
   int64_t auto_table_bytes = 12 << 20;  // automatic depth: prefix-table bytes per tile
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
+  int tile_mode = 0;                // 0 automatic, 1 shared-memory tiles, 2 global tiles
+  int64_t auto_global_table_bytes = 96 << 20;  // automatic depth, global tiles
+  int64_t global_table_entries = 32 << 20;     // list entries per table, global tiles
 };
 
 constexpr int32_t kNarrowMaxStates = 32767;  // 15-bit tile-local ids

@@ -118,9 +118,12 @@ class Tables:
     """Device-resident matching tables (group_graph.h:6-109, ngap.cu:3086-3111)."""
 
     def __init__(self, groups, device=0, precompute_depth=0, precompute_cutoff=-1,
-                 tile_states=0, max_table_entries=0):
+                 tile_states=0, max_table_entries=0, tile_mode="auto"):
+        modes = {"auto": 0, "shared": 1, "global": 2}
+        if tile_mode not in modes:
+            raise ValueError(f"tile_mode must be one of {sorted(modes)}")
         opts = _lib.TableOpts(device, precompute_depth, precompute_cutoff, tile_states,
-                              max_table_entries)
+                              max_table_entries, modes[tile_mode])
         h = ctypes.c_void_p()
         check(lib().ngap_tables_build(groups._h, ctypes.byref(opts), ctypes.byref(h)))
         self._h = h

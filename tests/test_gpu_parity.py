@@ -23,7 +23,8 @@ pytestmark = pytest.mark.gpu
 def run_both(engine, anml, data, num_seg, seg_len, group_num=1, depth=0, is_dup=False, **kw):
     nfa = nb.Nfa.from_string(anml)
     groups = nb.Groups(nfa, group_num=group_num)
-    tables = nb.Tables(groups, precompute_depth=depth, tile_states=kw.pop("tile_states", 0))
+    tables = nb.Tables(groups, precompute_depth=depth, tile_states=kw.pop("tile_states", 0),
+                       tile_mode=kw.pop("tile_mode", "auto"))
     got = engine.match(tables, data[:num_seg * seg_len], num_seg, seg_len, is_dup=is_dup, **kw)
     want, _ = oracle.match(groups.views(), data[:num_seg * seg_len], num_seg, seg_len,
                            is_dup=is_dup)
@@ -128,6 +129,24 @@ def test_sticky_report_and_start_states(engine):
             got, want = run_both(engine, w.text(), data, 4, 1250, group_num=2, depth=2,
                                  algorithm=algo, window=window)
             assert np.array_equal(got, want), (algo, window)
+
+
+@pytest.mark.parametrize("tile_mode,tile_states", [("shared", 0), ("global", 0), ("global", 2500)])
+@pytest.mark.parametrize("gen,kw,g,depth", [
+    (W.hamming_set, dict(seed=31, n_patterns=80, input_len=1 << 17, plant_every=1 << 10), 4, -1),
+    (W.levenshtein_set, dict(seed=32, n_patterns=40, input_len=1 << 16, plant_every=1 << 10), 3, 5),
+    (W.dotstar_set, dict(seed=33, n_patterns=80, input_len=1 << 16, plant_every=1 << 10), 2, 3),
+    (W.literal_set, dict(seed=34, input_len=1 << 16, plant_every=1 << 10), 2, -1),
+])
+def test_tile_modes(engine, tile_mode, tile_states, gen, kw, g, depth):
+    """Global tiles (CCs of several groups read through L2) and shared-memory
+    tiles give the same reports; a state cap splits global tiles across groups."""
+    anml, data = gen(**kw)
+    for algo in ("nonblockingpcgroups", "blockinggroups", "NAPgroups", "nonblockingallgroups"):
+        got, want = run_both(engine, anml, data, 2, len(data) // 2, group_num=g, depth=depth,
+                             algorithm=algo, tile_mode=tile_mode, tile_states=tile_states)
+        assert len(want) > 0
+        assert np.array_equal(got, want), algo
 
 
 @pytest.mark.parametrize("chunk,window,tile_states",[(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
