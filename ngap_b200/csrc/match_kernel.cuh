@@ -78,7 +78,10 @@ struct MatchParams {
   unsigned long long* work; // [0] entries expanded, [1] entries injected
 };
 
+// A window buffer: up to kMaxDepth - 1 look-behind bytes, 15 bytes of
+// alignment, W window bytes and one look-ahead byte.
 __host__ __device__ inline int window_buf_bytes(int W) { return ((W + 48) + 15) & ~15; }
+static_assert(kMaxDepth - 1 + 15 + 1 + 15 <= 48, "window buffer slack");
 
 __host__ __device__ inline int warp_smem_bytes(int W) {
   return kStackCap * 4 + 2 * window_buf_bytes(W) + kReportBuf * 8 + 3 * 32 * 4 + 16 +
@@ -144,9 +147,11 @@ __device__ __forceinline__ uint4 load_succ(const TileView& tv, uint32_t v) {
 
 // Everything about the current unit and window.
 struct UnitCtx {
-  const uint8_t* in;  // window symbols (class ids): in[0] = symbol at wb
+  const uint8_t* in;  // window symbols (class ids): in[0] = symbol at wb; in[-1 .. -(kMaxDepth-1)]
+                      // hold the look-behind bytes when the window is not the unit's first
   int64_t wb, hi, emit_lo;
   int wlen;
+  int iend;           // always-active injection covers window offsets below iend
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -447,7 +452,7 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
                                            int batch, int depth, unsigned long long& n_injected) {
   const TileDev& t = *tv.t;
   const int r = r0 + lane;
-  const bool valid = lane < batch && r < c.wlen;
+  const bool valid = lane < batch && r < c.iend;
   const int64_t q = c.wb + r;
   if (depth == 0) {  // scan the always-active list
     const uint32_t s = valid ? c.in[r] : 0u;
@@ -784,11 +789,15 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   unsigned long long n_expanded = 0, n_injected = 0;
   int staged = -1;  // tile whose image is in shared memory
 
-  auto issue = [&](int buf, int64_t wb, int64_t hi) {
+  // loads window [wb, min(wb + W, hi)) plus one look-ahead byte and `lb`
+  // look-behind bytes into buffer buf; returns the byte count, and in `skip`
+  // the offset of wb's byte in the buffer
+  auto issue = [&](int buf, int64_t wb, int64_t hi, int lb, uint32_t& skip) {
     const int64_t we = min(wb + (int64_t)W, hi);
-    const int64_t end = min(we + 1, hi);  // window bytes plus one look-ahead byte
-    const int64_t a0 = wb & ~(int64_t)15;
+    const int64_t end = min(we + 1, hi);
+    const int64_t a0 = (wb - lb) & ~(int64_t)15;
     const uint32_t bytes = (uint32_t)(((end - a0) + 15) & ~(int64_t)15);
+    skip = (uint32_t)(wb - a0);
     if (lane == 0) {
       mbar_expect_tx(&ws.bar[buf], bytes);
       bulk_g2s(ws.in[buf], p.input + a0, bytes, &ws.bar[buf]);
@@ -837,6 +846,10 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
     const bool translate = t->cw != 8;
+    // Without sticky states, the last depth - 1 positions of a window are
+    // injected at the start of the next one (from look-behind bytes), so that
+    // every position but the unit's last ones gets the full table depth.
+    const int defer = (depth > 1 && !tv.sticky) ? depth - 1 : 0;
 
     while (!dead) {
       unsigned uid = 0;
@@ -851,12 +864,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       w.key_hi = un.key_hi;
       w.base = (uint32_t)un.base;
       int cur = 0;
-      uint32_t nbytes[2];
-      nbytes[0] = issue(0, un.lo, c.hi);
+      uint32_t nbytes[2], skip[2];
+      nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
+      int64_t inj_pos = un.lo;  // next position for always-active injection
       for (int64_t wb = un.lo; wb < c.hi; wb += W) {
         const int64_t we = min(wb + (int64_t)W, c.hi);
         c.wb = wb;
         c.wlen = (int)(we - wb);
+        c.iend = we == c.hi ? c.wlen : c.wlen - defer;
         if (!mbar_wait(&ws.bar[cur], phase[cur])) {
           if (lane == 0) atomicOr(p.err, kErrTimeout);
           dead = true;
@@ -868,8 +883,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
           for (uint32_t i = lane; i < nbytes[cur]; i += 32) ws.in[cur][i] = tv.cls[ws.in[cur][i]];
         }
         __syncwarp();
-        if (we < c.hi) nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi);
-        c.in = ws.in[cur] + (wb & 15);
+        if (we < c.hi)
+          nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi, (int)min((int64_t)defer, we - un.lo), skip[cur ^ 1]);
+        c.in = ws.in[cur] + skip[cur];
         // carried states: matched at wb
         w.top = 0;
         if (w.ncarry > 0) {
@@ -900,11 +916,13 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
             push_entry(p, ws, w, lane, need && !reg, v << kEntryPosBits);
           }
         }
-        int cursor = 0;  // next window offset to inject
+        // next window offset to inject: negative for positions deferred from
+        // the previous window (at most `defer` of them)
+        int cursor = (int)(inj_pos - wb);
         while (true) {
           // inject only when the overflow stack is empty, so that it holds at
           // most one batch's excess
-          if (w.top < kInjectLow && w.ovf_n == 0 && cursor < c.wlen) {
+          if (w.top < kInjectLow && w.ovf_n == 0 && cursor < c.iend) {
             inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
             cursor += batch;
             continue;
@@ -918,11 +936,12 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
               __syncwarp();
               continue;
             }
-            if (cursor < c.wlen) continue;
+            if (cursor < c.iend) continue;
             break;
           }
           expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
         }
+        inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
         cur ^= 1;
       }
       if (dead) {

@@ -149,6 +149,20 @@ def test_tile_modes(engine, tile_mode, tile_states, gen, kw, g, depth):
         assert np.array_equal(got, want), algo
 
 
+@pytest.mark.parametrize("window,chunk", [(3, 0), (5, 100), (10, 0), (64, 333), (1000, 0)])
+@pytest.mark.parametrize("tile_mode", ["shared", "global"])
+def test_deferred_window_tail(engine, window, chunk, tile_mode):
+    """Deep tables: the last depth - 1 positions of a window are injected from
+    the next window's look-behind bytes, also when windows are shorter than that."""
+    anml, data = W.hamming_set(seed=35, n_patterns=50, input_len=1 << 15, plant_every=1 << 9)
+    for depth in (8, 12):
+        got, want = run_both(engine, anml, data, 3, len(data) // 3, group_num=2, depth=depth,
+                             algorithm="nonblockingpcgroups", window=window, chunk=chunk,
+                             tile_mode=tile_mode)
+        assert len(want) > 10
+        assert np.array_equal(got, want), depth
+
+
 @pytest.mark.parametrize("chunk,window,tile_states",[(100, 128, 0), (1000, 0, 64), (0, 33, 300)])
 def test_chunking_and_tiling(engine, chunk, window, tile_states):
     """Small chunks, windows and tiles exercise warm-up, carry and tile splits."""
