@@ -29,6 +29,12 @@ namespace {
     }                                                                                      \
   } while (0)
 
+// Device counters of an engine: [0] raw reports, [1] unique reports, [2..3]
+// work, [5..6] the standalone sort's counts, [kRadixCount] keys left to the
+// radix pipeline after the small-set sort.
+constexpr int kNumCounters = 16;
+constexpr int kRadixCount = 8;
+
 int bits_for(uint64_t x) {  // bits needed to hold values < x (x >= 1)
   int b = 0;
   while (b < 64 && (x - 1) >> b) b++;
@@ -36,6 +42,20 @@ int bits_for(uint64_t x) {  // bits needed to hold values < x (x >= 1)
 }
 
 }  // namespace
+
+// A report sort captured as a CUDA graph (see sort_reports).
+struct SortGraph {
+  std::vector<uint64_t> key;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  int chain = 0;  // kernels in the conditional radix pipeline
+  void release() {
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    ge = nullptr;
+    g = nullptr;
+  }
+};
 
 struct ngap_tables {
   int device = 0;
@@ -103,7 +123,8 @@ struct ngap_engine {
   unsigned long long* d_counters = nullptr;
   int* d_err = nullptr;
   unsigned int* d_unit_counter = nullptr;
-  unsigned long long* h_counters = nullptr;  // pinned mirror (4 counters + err)
+  unsigned long long* h_counters = nullptr;  // pinned mirror: [0..3] counters, [4] err,
+                                             // [kRadixCount] keys left to the radix pipeline
   // per-warp scratch
   uint32_t* d_carry = nullptr;
   uint32_t* d_marks = nullptr;
@@ -130,6 +151,11 @@ struct ngap_engine {
   int graph_launches = 0;
   cudaStream_t cap_stream = nullptr;  // capture/replay stream of the batched graph
   cudaEvent_t cap_ev[2] = {nullptr, nullptr};
+  // report sorts as graphs with a conditional radix pipeline, per configuration
+  std::vector<SortGraph> sort_graphs;
+  cudaStream_t sort_cs = nullptr;     // capture stream of those graphs
+  bool sort_graph_off = false;
+  int sort_chain_pending = 0;         // pipeline kernels of the last graph sort, if it ran
 
   ~ngap_engine() {
     cudaFree(d_input);
@@ -147,6 +173,8 @@ struct ngap_engine {
     cudaFree(d_ovf);
     cudaFree(d_stream_ids);
     if (graph) cudaGraphExecDestroy(graph);
+    for (auto& g : sort_graphs) g.release();
+    if (sort_cs) cudaStreamDestroy(sort_cs);
     for (auto& c : cap_ev)
       if (c) cudaEventDestroy(c);
     if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -263,10 +291,14 @@ int ngap_engine_create(int device, ngap_engine** out) {
   std::unique_ptr<ngap_engine> e(new ngap_engine());
   e->device = device;
   CUDA_TRY(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device));
-  CUDA_TRY(cudaMalloc(&e->d_counters, 8 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMalloc(&e->d_counters, kNumCounters * sizeof(unsigned long long)));
+  CUDA_TRY(cudaFuncSetAttribute(small_sort_unique<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSmallSortSmem));
+  CUDA_TRY(cudaFuncSetAttribute(small_sort_unique<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSmallSortSmem));
   CUDA_TRY(cudaMalloc(&e->d_err, sizeof(int)));
   CUDA_TRY(cudaMalloc(&e->d_unit_counter, sizeof(unsigned int)));
-  CUDA_TRY(cudaMallocHost(&e->h_counters, 8 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMallocHost(&e->h_counters, kNumCounters * sizeof(unsigned long long)));
   for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
   *out = e.release();
   return NGAP_OK;
@@ -451,32 +483,172 @@ int launch_match(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t s
   return NGAP_OK;
 }
 
+// One sort of report keys: d_in[0 .. *d_n) (clamped to cap) into unique
+// reports at d_out (and stream indices at d_out_stream for MODE 1).
+//   MODE 0: keys offset << 32 | id, written as id << 32 | offset;
+//   MODE 1: keys stream << sshift | offset << oshift | id (batched matching).
+// shifts: the 4-bit digits the radix pipeline sorts, least significant first.
+struct SortJob {
+  int mode;
+  uint64_t* d_in;
+  const unsigned long long* d_n;
+  uint64_t cap;
+  std::vector<int> shifts;
+  int oshift, sshift;
+  uint64_t* d_out;
+  uint32_t* d_out_stream;
+  unsigned long long* d_unique_n;
+};
+
+// The radix pipeline over *radix_n keys; kernels counts its launches.
+int radix_chain(ngap_engine* e, const SortJob& j, const unsigned long long* radix_n,
+                cudaStream_t st, int* kernels) {
+  const uint32_t max_tiles = (uint32_t)((j.cap + kSortTile - 1) / kSortTile);
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, e->num_sms * 8));
+  // ping-pong between d_in (an engine-owned buffer) and d_tmp
+  uint64_t* src = j.d_in;
+  uint64_t* dst = e->d_tmp;
+  int k = 0;
+  for (int sh : j.shifts) {
+    radix_hist<<<grid, kSortThreads, 0, st>>>(src, radix_n, j.cap, sh, e->d_hist);
+    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, radix_n, j.cap, 16, nullptr);
+    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, radix_n, j.cap, sh, e->d_hist);
+    k += 3;
+    std::swap(src, dst);
+  }
+  unique_count<<<grid, kSortThreads, 0, st>>>(src, radix_n, j.cap, e->d_hist);
+  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, radix_n, j.cap, 1, j.d_unique_n);
+  if (j.mode == 0)
+    unique_write<<<grid, kSortThreads, 0, st>>>(src, radix_n, j.cap, e->d_hist, j.d_out);
+  else
+    unique_write_fields<<<grid, kSortThreads, 0, st>>>(src, radix_n, j.cap, e->d_hist, j.oshift,
+                                                       j.sshift, j.d_out, j.d_out_stream);
+  k += 3;
+  *kernels = k;
+  CUDA_TRY(cudaGetLastError());
+  return NGAP_OK;
+}
+
+void* small_kernel(int mode) {
+  return mode == 0 ? reinterpret_cast<void*>(small_sort_unique<0>)
+                   : reinterpret_cast<void*>(small_sort_unique<1>);
+}
+
+// Builds the graph: the small-set kernel, then the radix pipeline in the body
+// of a conditional (IF) node whose condition the small-set kernel sets when
+// it leaves keys to the pipeline.
+int build_sort_graph(ngap_engine* e, const SortJob& j, SortGraph& sg) {
+  if (!e->sort_cs) CUDA_TRY(cudaStreamCreateWithFlags(&e->sort_cs, cudaStreamNonBlocking));
+  CUDA_TRY(cudaGraphCreate(&sg.g, 0));
+  cudaGraphConditionalHandle h = 0;
+  CUDA_TRY(cudaGraphConditionalHandleCreate(&h, sg.g, 0, cudaGraphCondAssignDefault));
+  unsigned long long* radix_n = e->d_counters + kRadixCount;
+  uint64_t* d_in = j.d_in;
+  const unsigned long long* d_n = j.d_n;
+  uint64_t cap = j.cap;
+  unsigned long long* d_unique_n = j.d_unique_n;
+  int oshift = j.oshift, sshift = j.sshift;
+  uint64_t* d_out = j.d_out;
+  uint32_t* d_out_stream = j.d_out_stream;
+  int set_cond = 1;
+  void* args[] = {&d_in, &d_n, &cap, &radix_n, &d_unique_n, &oshift, &sshift, &d_out,
+                  &d_out_stream, &h, &set_cond};
+  cudaKernelNodeParams kp = {};
+  kp.func = small_kernel(j.mode);
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(kSmallThreads);
+  kp.sharedMemBytes = kSmallSortSmem;
+  kp.kernelParams = args;
+  cudaGraphNode_t kn = nullptr, cn = nullptr;
+  CUDA_TRY(cudaGraphAddKernelNode(&kn, sg.g, nullptr, 0, &kp));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  CUDA_TRY(cudaGraphAddNode(&cn, sg.g, &kn, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CUDA_TRY(cudaStreamBeginCaptureToGraph(e->sort_cs, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  int kernels = 0;
+  const int rc = radix_chain(e, j, radix_n, e->sort_cs, &kernels);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(e->sort_cs, &captured);
+  if (rc != NGAP_OK) return rc;
+  CUDA_TRY(ce);
+  CUDA_TRY(cudaGraphInstantiate(&sg.ge, sg.g, 0));
+  sg.chain = kernels;
+  return NGAP_OK;
+}
+
+// Enqueues a sort on st. Outside stream capture it replays a cached graph
+// (one launch; the radix pipeline runs only for more than kSmallSort keys);
+// inside a capture, or where graphs are unavailable, it launches the small-set
+// kernel and the pipeline, whose kernels find no keys after a small set.
+int sort_reports(ngap_engine* e, const SortJob& j, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs == cudaStreamCaptureStatusNone && !e->sort_graph_off) {
+    std::vector<uint64_t> key = {(uint64_t)j.mode,   (uint64_t)(uintptr_t)j.d_in,
+                                 (uint64_t)(uintptr_t)j.d_n, j.cap,
+                                 (uint64_t)j.oshift, (uint64_t)j.sshift,
+                                 (uint64_t)(uintptr_t)j.d_out,
+                                 (uint64_t)(uintptr_t)j.d_out_stream,
+                                 (uint64_t)(uintptr_t)j.d_unique_n,
+                                 (uint64_t)(uintptr_t)e->d_tmp, (uint64_t)(uintptr_t)e->d_hist};
+    for (int sh : j.shifts) key.push_back((uint64_t)sh);
+    SortGraph* sg = nullptr;
+    for (auto& g : e->sort_graphs)
+      if (g.key == key) sg = &g;
+    if (!sg) {
+      if (e->sort_graphs.size() >= 8) {  // keep a few configurations
+        e->sort_graphs.front().release();
+        e->sort_graphs.erase(e->sort_graphs.begin());
+      }
+      SortGraph ng;
+      ng.key = key;
+      if (build_sort_graph(e, j, ng) == NGAP_OK) {
+        e->sort_graphs.push_back(ng);
+        sg = &e->sort_graphs.back();
+      } else {  // graphs unavailable here: launch the kernels directly from now on
+        ng.release();
+        cudaGetLastError();
+        e->sort_graph_off = true;
+      }
+    }
+    if (sg) {
+      CUDA_TRY(cudaGraphLaunch(sg->ge, st));
+      e->launches++;
+      e->sort_chain_pending = sg->chain;
+      return NGAP_OK;
+    }
+  }
+  unsigned long long* radix_n = e->d_counters + kRadixCount;
+  const cudaGraphConditionalHandle none = 0;
+  const int set_cond = 0;
+  if (j.mode == 0)
+    small_sort_unique<0><<<1, kSmallThreads, kSmallSortSmem, st>>>(
+        j.d_in, j.d_n, j.cap, radix_n, j.d_unique_n, j.oshift, j.sshift, j.d_out, j.d_out_stream,
+        none, set_cond);
+  else
+    small_sort_unique<1><<<1, kSmallThreads, kSmallSortSmem, st>>>(
+        j.d_in, j.d_n, j.cap, radix_n, j.d_unique_n, j.oshift, j.sshift, j.d_out, j.d_out_stream,
+        none, set_cond);
+  int kernels = 0;
+  const int rc = radix_chain(e, j, radix_n, st, &kernels);
+  e->launches += 1 + kernels;
+  return rc;
+}
+
 // Sorts d_in[0 .. *d_n) (clamped to cap) into d_out as unique reference-encoded
 // reports; *d_unique_n receives the count. off_bits / id_bits bound the key.
 int sort_unique(ngap_engine* e, uint64_t* d_in, const unsigned long long* d_n, uint64_t cap,
                 int off_bits, int id_bits, uint64_t* d_out, unsigned long long* d_unique_n,
                 cudaStream_t st) {
-  const uint32_t max_tiles = (uint32_t)((cap + kSortTile - 1) / kSortTile);
-  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, e->num_sms * 8));
-  std::vector<int> shifts;
-  for (int b = 0; b < id_bits; b += 4) shifts.push_back(b);
-  for (int b = 0; b < off_bits; b += 4) shifts.push_back(32 + b);
-  // ping-pong between d_in (an engine-owned buffer) and d_tmp
-  uint64_t* src = d_in;
-  uint64_t* dst = e->d_tmp;
-  for (int sh : shifts) {
-    radix_hist<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, sh, e->d_hist);
-    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 16, nullptr);
-    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, d_n, cap, sh, e->d_hist);
-    e->launches += 3;
-    std::swap(src, dst);
-  }
-  unique_count<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist);
-  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 1, d_unique_n);
-  unique_write<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist, d_out);
-  e->launches += 3;
-  CUDA_TRY(cudaGetLastError());
-  return NGAP_OK;
+  SortJob j{0, d_in, d_n, cap, {}, 32, 64, d_out, nullptr, d_unique_n};
+  for (int b = 0; b < id_bits; b += 4) j.shifts.push_back(b);
+  for (int b = 0; b < off_bits; b += 4) j.shifts.push_back(32 + b);
+  return sort_reports(e, j, st);
 }
 
 // Batched keys stream << sshift | offset << oshift | id: radix passes over the
@@ -484,28 +656,12 @@ int sort_unique(ngap_engine* e, uint64_t* d_in, const unsigned long long* d_n, u
 int sort_unique_fields(ngap_engine* e, const unsigned long long* d_n, uint64_t cap, int ibits,
                        int oshift, int obits, int sshift, int sbits,
                        unsigned long long* d_unique_n, cudaStream_t st) {
-  const uint32_t max_tiles = (uint32_t)((cap + kSortTile - 1) / kSortTile);
-  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, e->num_sms * 8));
-  std::vector<int> shifts;
-  for (int b = 0; b < ibits; b += 4) shifts.push_back(b);
-  for (int b = 0; b < obits; b += 4) shifts.push_back(oshift + b);
-  for (int b = 0; b < sbits; b += 4) shifts.push_back(sshift + b);
-  uint64_t* src = e->d_reports;
-  uint64_t* dst = e->d_tmp;
-  for (int sh : shifts) {
-    radix_hist<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, sh, e->d_hist);
-    scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 16, nullptr);
-    radix_scatter<<<grid, kSortThreads, 0, st>>>(src, dst, d_n, cap, sh, e->d_hist);
-    e->launches += 3;
-    std::swap(src, dst);
-  }
-  unique_count<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist);
-  scan_exclusive_1block<<<1, kScanThreads, 0, st>>>(e->d_hist, d_n, cap, 1, d_unique_n);
-  unique_write_fields<<<grid, kSortThreads, 0, st>>>(src, d_n, cap, e->d_hist, oshift, sshift,
-                                                     e->d_unique, e->d_stream_ids);
-  e->launches += 3;
-  CUDA_TRY(cudaGetLastError());
-  return NGAP_OK;
+  SortJob j{1, e->d_reports, d_n, cap, {}, oshift, sshift, e->d_unique, e->d_stream_ids,
+            d_unique_n};
+  for (int b = 0; b < ibits; b += 4) j.shifts.push_back(b);
+  for (int b = 0; b < obits; b += 4) j.shifts.push_back(oshift + b);
+  for (int b = 0; b < sbits; b += 4) j.shifts.push_back(sshift + b);
+  return sort_reports(e, j, st);
 }
 
 // --algorithm -> prefix depth, privatization and window.
@@ -553,6 +709,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   e->stream = st;
   e->launches = 0;
+  e->sort_chain_pending = 0;
   e->ran = false;
   int algo = p->algorithm;
   int depth = 1, priv = 0, window = p->window > 0 ? p->window : 1024;
@@ -684,6 +841,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   CUDA_TRY(cudaMemcpyAsync(e->h_counters, e->d_counters, 4 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaMemcpyAsync(e->h_counters + 4, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(e->h_counters + kRadixCount, e->d_counters + kRadixCount,
+                           sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   e->ran = true;
   return NGAP_OK;
 }
@@ -697,6 +856,9 @@ int ngap_engine_sync(ngap_engine* e) {
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   CUDA_TRY(cudaEventElapsedTime(&e->match_ms, e->ev[1], e->ev[2]));
   CUDA_TRY(cudaEventElapsedTime(&e->sort_ms, e->ev[2], e->ev[3]));
+  if (e->sort_chain_pending > 0 && e->h_counters[kRadixCount] > 0)  // the radix pipeline ran
+    e->launches += e->sort_chain_pending;
+  e->sort_chain_pending = 0;
   int err = (int)(e->h_counters[4] & 0xffffffffull);
   if (err & kErrTimeout) {
     set_error("a bounded device wait gave up; results are incomplete");
@@ -1007,10 +1169,13 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     CUDA_TRY(cudaMemcpyAsync(e->h_counters, e->d_counters, 4 * sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost, qs));
     CUDA_TRY(cudaMemcpyAsync(e->h_counters + 4, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, qs));
+    CUDA_TRY(cudaMemcpyAsync(e->h_counters + kRadixCount, e->d_counters + kRadixCount,
+                             sizeof(unsigned long long), cudaMemcpyDeviceToHost, qs));
     return NGAP_OK;
   };
 
   e->launches = 0;
+  e->sort_chain_pending = 0;
   if (!p->use_graph) {
     e->graph_mode = false;
     CUDA_TRY(cudaEventRecord(e->ev[0], st));

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_exclusive_1block(uint32_t* 
     a[i] = run;
     run += x;
   }
-  if (total && threadIdx.x == kScanThreads - 1) *total = part[kScanThreads - 1];
+  if (total && n > 0 && threadIdx.x == kScanThreads - 1) *total = part[kScanThreads - 1];
 }
 
 // Stable scatter of one digit pass. offs = scanned hist (digit-major).
@@ -261,6 +261,85 @@ __global__ void __launch_bounds__(kSortThreads) unique_write_fields(
     }
     __syncthreads();
   }
+}
+
+// Small report sets: one CTA sorts and deduplicates up to kSmallSort keys in
+// shared memory (bitonic sort over the next power of two, padded with
+// all-ones keys, which sort last), then writes the unique reports like
+// unique_write (MODE 0) or unique_write_fields (MODE 1). It stores in
+// *radix_n the key count the radix pipeline still has to sort: 0 when the
+// keys were handled here (the pipeline's kernels then find no tiles), n
+// otherwise; launched from a graph, it also sets the condition of the
+// conditional node that holds the pipeline.
+constexpr int kSmallSort = 8192;
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallSortSmem = kSmallSort * 8;
+
+template <int MODE>
+__global__ void __launch_bounds__(kSmallThreads) small_sort_unique(
+    const uint64_t* __restrict__ keys, const unsigned long long* d_n, uint64_t cap,
+    unsigned long long* radix_n, unsigned long long* d_unique_n, int oshift, int sshift,
+    uint64_t* __restrict__ out, uint32_t* __restrict__ out_stream, cudaGraphConditionalHandle cond,
+    int set_cond) {
+  extern __shared__ __align__(16) uint64_t sk[];
+  __shared__ uint32_t wsum[kSmallThreads / 32];
+  const uint64_t n = dev_count(d_n, cap);
+  const bool big = n > (uint64_t)kSmallSort;
+  if (threadIdx.x == 0) {
+    *radix_n = big ? n : 0ull;
+    if (set_cond) cudaGraphSetConditional(cond, big ? 1u : 0u);  // graph launches only
+  }
+  if (big) return;
+  const uint32_t nn = (uint32_t)n;
+  uint32_t m = 1;
+  while (m < nn) m <<= 1;
+  for (uint32_t i = threadIdx.x; i < m; i += kSmallThreads) sk[i] = i < nn ? keys[i] : ~0ull;
+  __syncthreads();
+  for (uint32_t k = 2; k <= m; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < m; i += kSmallThreads) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint64_t a = sk[i], b = sk[l];
+          if ((a > b) == ((i & k) == 0)) {
+            sk[i] = b;
+            sk[l] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // first key of every run, compacted in order: thread t owns [b, e)
+  const uint32_t per = (nn + kSmallThreads - 1) / kSmallThreads;
+  const uint32_t b = min(threadIdx.x * per, nn), e = min(b + per, nn);
+  uint32_t c = 0;
+  for (uint32_t i = b; i < e; i++) c += (i == 0 || sk[i] != sk[i - 1]) ? 1u : 0u;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  uint32_t pos = incl - c;
+  for (int i = 0; i < warp; i++) pos += wsum[i];
+  for (uint32_t i = b; i < e; i++) {
+    if (!(i == 0 || sk[i] != sk[i - 1])) continue;
+    const uint64_t key = sk[i];
+    if (MODE == 0) {
+      out[pos] = (key << 32) | (key >> 32);
+    } else {
+      const uint64_t id = key & ((1ull << oshift) - 1);
+      const uint64_t off = (key >> oshift) & ((1ull << (sshift - oshift)) - 1);
+      out[pos] = (id << 32) | off;
+      out_stream[pos] = sshift < 64 ? (uint32_t)(key >> sshift) : 0u;
+    }
+    pos++;
+  }
+  if (threadIdx.x == kSmallThreads - 1) *d_unique_n = pos;
 }
 
 }  // namespace ngap

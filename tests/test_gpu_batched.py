@@ -77,3 +77,42 @@ def test_plain_after_batched(engine, suite):
     got = engine.match(t, seg, 4, 1024)
     want, _ = oracle.match(groups[0].views(), seg, 4, 1024)
     assert np.array_equal(got, want)
+
+
+def test_batched_global_tiles(engine, suite):
+    """Global tiles (several groups per tile) inside a tableset."""
+    nfas, data, offsets, lengths, nfa_of, groups = suite
+    tables = [nb.Tables(g, precompute_depth=-1, tile_mode="global") for g in groups]
+    ts = nb.TableSet(tables)
+    nb.batch_match_async(engine, ts, data, offsets, lengths, nfa_of, window=200)
+    engine.sync()
+    reps, sids = nb.batch_results(engine)
+    got = nb.split_by_stream(reps, sids, len(offsets))
+    for s, w in enumerate(_expected(suite)):
+        assert np.array_equal(got[s], w), s
+
+
+def test_batched_dense_reports(engine):
+    """Tens of thousands of reports over many streams: the radix pipeline."""
+    w = W.AnmlWriter()
+    w.ste("a", list(range(1, 256)), ["b"], start="all-input", report=True)
+    w.ste("b", [ord("x")], [], report=True)
+    g = nb.Groups(nb.Nfa.from_string(w.text()), group_num=1)
+    ts = nb.TableSet([nb.Tables(g, precompute_depth=2)])
+    rng = np.random.default_rng(5)
+    lengths = rng.integers(0, 3000, size=40).astype(np.uint64)
+    offsets = np.concatenate([[0], np.cumsum(lengths)[:-1]]).astype(np.uint64)
+    data = rng.integers(0, 256, size=int(lengths.sum()), dtype=np.uint8)
+    nfa_of = np.zeros(len(lengths), np.int32)
+    nb.batch_match_async(engine, ts, data, offsets, lengths, nfa_of)
+    engine.sync()
+    reps, sids = nb.batch_results(engine)
+    got = nb.split_by_stream(reps, sids, len(offsets))
+    total = 0
+    for s in range(len(lengths)):
+        seg = data[int(offsets[s]):int(offsets[s] + lengths[s])]
+        want = (oracle.match(g.views(), seg, 1, int(lengths[s]))[0] if lengths[s]
+                else np.zeros(0, np.uint64))
+        total += len(want)
+        assert np.array_equal(got[s], want), s
+    assert total > 20000

@@ -240,3 +240,39 @@ def test_device_input_and_sort_api(engine):
     torch.cuda.synchronize()
     assert n == len(want)
     assert np.array_equal(dout[:n].cpu().numpy().view(np.uint64), want)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5000, 8192, 8193, 60000])
+def test_sort_unique_sizes(engine, n):
+    """Device sort + unique on both sides of the single-CTA cutoff (8192 keys)."""
+    import torch
+    rng = np.random.default_rng(n)
+    ids = rng.integers(0, 1 << 24, size=n, dtype=np.uint64)
+    offs = rng.integers(0, 1 << 30, size=n, dtype=np.uint64)
+    keys = (ids << np.uint64(32)) | offs
+    keys = np.concatenate([keys, keys[: n // 3]])
+    rng.shuffle(keys)
+    swapped = np.unique((keys << np.uint64(32)) | (keys >> np.uint64(32)))
+    want = (swapped << np.uint64(32)) | (swapped >> np.uint64(32))
+    din = torch.from_numpy(keys.view(np.int64)).cuda()
+    dout = torch.empty_like(din)
+    m = engine.sort_unique_device(din.data_ptr(), len(keys), dout.data_ptr())
+    torch.cuda.synchronize()
+    assert m == len(want)
+    assert np.array_equal(dout[:m].cpu().numpy().view(np.uint64), want)
+
+
+@pytest.mark.parametrize("algo", ["nonblockingpcgroups", "NAPgroups"])
+def test_dense_reports(engine, algo):
+    """A report at almost every position: tens of thousands of reports take the
+    radix pipeline, a handful the single-CTA sort."""
+    w = W.AnmlWriter()
+    w.ste("a", list(range(1, 256)), ["b"], start="all-input", report=True)
+    w.ste("b", [ord("x")], [], report=True)
+    rng = np.random.default_rng(4)
+    for size in (40000, 3000):
+        data = rng.integers(0, 256, size=size, dtype=np.uint8)
+        got, want = run_both(engine, w.text(), data, 4, size // 4, group_num=1, depth=2,
+                             algorithm=algo)
+        assert len(want) > size // 2
+        assert np.array_equal(got, want), size
