@@ -70,6 +70,9 @@ struct TileDev {
   int32_t inj_batch0 = 32;  // the same when the always-active list is scanned
   int32_t nsticky = 0;      // sticky states (bitmap at off_sticky in the image)
   int32_t off_sticky = 0;
+  int32_t phase = 0;        // 0 plain; 1 activation pass; 2 layered (sticky states pre-registered)
+  int32_t nact = 0;         // activation slots per segment (phase 1 and 2)
+  const uint32_t* act_local = nullptr;  // phase 2: [nact] local id of each slot's sticky state
   const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
   const uint32_t* sid = nullptr;    // [nstates] local -> report id (sid | group << 22)
   const uint32_t* aas = nullptr;    // [naas] local ids
@@ -80,13 +83,17 @@ struct TileDev {
 // A unit of work: one tile over input positions [lo, hi); reports are kept for
 // positions >= emit_lo (the positions before are warm-up of a chunk). A report
 // at position q is stored as key_hi | (q - base) << off_shift | id, where
-// key_hi carries the stream index in batched matching (0 otherwise).
+// key_hi carries the stream index in batched matching (0 otherwise). Units of
+// activation tiles record the first match of sticky state slot i of their
+// segment as atomicMin(act[act_row + i], q - base); units of the paired
+// layered tile read those slots.
 struct UnitDev {
   int32_t tile;
   uint32_t flags;  // bit0: inject start-of-data states at lo
   int64_t lo, hi, emit_lo;
   int64_t base;      // first byte of the unit's stream
   uint64_t key_hi;   // stream index, already shifted into the report key
+  int64_t act_row;   // phase 1 and 2 tiles: first activation slot of the unit's segment
 };
 
 // A CTA-level task: consecutive units [ubegin, uend) of one tile.

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -57,7 +58,12 @@ struct SortGraph {
   }
 };
 
+// Plan caches key on these serial numbers, not on addresses: a new object
+// may be allocated where a destroyed one was.
+std::atomic<uint64_t> g_next_serial{1};
+
 struct ngap_tables {
+  uint64_t serial = g_next_serial.fetch_add(1);
   int device = 0;
   int num_groups = 0;
   std::vector<TileHost> tiles;
@@ -67,6 +73,8 @@ struct ngap_tables {
   int64_t bytes = 0;
   int32_t max_states = 0;
   int32_t image_region = 0;  // shared-memory bytes reserved for tile images
+  std::vector<int32_t> pair_nact;  // activation slots of each (activation, layered) tile pair
+  int32_t max_nact = 0;            // largest pair
 
   ~ngap_tables() {
     for (void* p : allocs) cudaFree(p);
@@ -104,7 +112,7 @@ struct ngap_engine {
   uint8_t* d_input = nullptr;
   size_t input_cap = 0;
   // units (cached plan for one tables object)
-  const ngap_tables* plan_tables = nullptr;
+  uint64_t plan_tables = 0;  // serial of the tables the plain plan was made for
   UnitPlanKey plan_key{-1, -1, -1, -1, -1, -1};
   UnitDev* d_units = nullptr;
   size_t units_cap = 0;
@@ -112,6 +120,12 @@ struct ngap_engine {
   TaskDev* d_tasks = nullptr;
   size_t tasks_cap = 0;
   int32_t ntasks = 0;
+  int32_t ntasks1 = 0;       // tasks of activation tiles, launched first
+  int64_t act_entries = 0;   // activation slots the plan uses
+  uint32_t* d_act = nullptr;
+  int64_t act_cap = 0;
+  uint32_t* d_stk = nullptr; // per-slot sticky lists of layered units (beyond shared memory)
+  int stk_cap = 0;
   // reports
   uint64_t rep_cap = 0;
   uint64_t* d_reports = nullptr;
@@ -140,7 +154,7 @@ struct ngap_engine {
   bool ran = false;
   int grid = 0;
   // batched matching
-  const void* batch_ts = nullptr;
+  uint64_t batch_ts = 0;     // serial of the tableset the batched plan was made for
   std::vector<ngap_batch_stream> batch_streams;
   int batch_window = -1, batch_chunk = -1;
   uint32_t* d_stream_ids = nullptr;
@@ -171,6 +185,8 @@ struct ngap_engine {
     cudaFree(d_carry);
     cudaFree(d_marks);
     cudaFree(d_ovf);
+    cudaFree(d_act);
+    cudaFree(d_stk);
     cudaFree(d_stream_ids);
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& g : sort_graphs) g.release();
@@ -241,6 +257,14 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.inj_batch0 = th.inj_batch0;
     d.nsticky = th.nsticky;
     d.off_sticky = th.off_sticky;
+    d.phase = th.phase;
+    d.nact = th.nact;
+    if (th.pair >= 0) {
+      if ((int)t->pair_nact.size() <= th.pair) t->pair_nact.resize(th.pair + 1, 0);
+      t->pair_nact[th.pair] = th.nact;
+      t->max_nact = std::max(t->max_nact, th.nact);
+    }
+    if ((rc = t->upload(th.act_local, &d.act_local)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.image, &d.image)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.sid, &d.sid)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.aas, &d.aas)) != NGAP_OK) return rc;
@@ -334,17 +358,31 @@ int ensure_reports(ngap_engine* e, uint64_t cap) {
   return NGAP_OK;
 }
 
-int ensure_slots(ngap_engine* e, size_t slots, int max_states) {
+int ensure_slots(ngap_engine* e, size_t slots, int max_states, int max_nact) {
   int carry_cap = std::max(max_states, 32);
   int mark_words = (max_states + 31) / 32 + 1;
   int ovf_cap = 1 << 16;
+  const int stk_cap = max_nact > kStickyCap ? max_nact : 0;
+  if (slots <= e->slots && stk_cap > e->stk_cap) {  // only the sticky lists grow
+    cudaFree(e->d_stk);
+    e->d_stk = nullptr;
+    e->stk_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_stk, e->slots * 2 * (size_t)stk_cap * sizeof(uint32_t)));
+    e->stk_cap = stk_cap;
+  }
   if (slots <= e->slots && carry_cap <= e->carry_cap && mark_words <= e->mark_words) return NGAP_OK;
   cudaFree(e->d_carry);
   cudaFree(e->d_marks);
   cudaFree(e->d_ovf);
-  e->d_carry = e->d_marks = e->d_ovf = nullptr;
-  e->slots = 0;
+  cudaFree(e->d_stk);
+  e->d_carry = e->d_marks = e->d_ovf = e->d_stk = nullptr;
+  e->stk_cap = 0;
   slots = std::max(slots, e->slots);
+  e->slots = 0;
+  if (stk_cap > 0) {
+    CUDA_TRY(cudaMalloc(&e->d_stk, slots * 2 * (size_t)stk_cap * sizeof(uint32_t)));
+    e->stk_cap = stk_cap;
+  }
   CUDA_TRY(cudaMalloc(&e->d_carry, slots * (size_t)carry_cap * sizeof(uint32_t)));
   CUDA_TRY(cudaMalloc(&e->d_marks, slots * (size_t)mark_words * sizeof(uint32_t)));
   CUDA_TRY(cudaMemset(e->d_marks, 0, slots * (size_t)mark_words * sizeof(uint32_t)));
@@ -371,11 +409,14 @@ struct SegSpec {
 };
 
 void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int chunk_opt,
-               std::vector<UnitDev>& unbounded, std::vector<UnitDev>& bounded) {
+               int64_t act_row, std::vector<UnitDev>& pass1, std::vector<UnitDev>& unbounded,
+               std::vector<UnitDev>& bounded) {
   UnitDev u{};
   u.tile = tile;
   u.key_hi = s.key_hi;
   u.base = s.base;
+  u.act_row = act_row;
+  std::vector<UnitDev>& chunks = th.phase == 1 ? pass1 : bounded;
   const bool starts = s.starts && !th.start.empty();
   if (th.max_path < 0) {
     u.flags = starts ? 1u : 0u;
@@ -396,22 +437,46 @@ void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int c
     u.hi = std::min(em + chunk, s.hi);
     u.emit_lo = em;
     u.flags = (starts && u.lo == s.lo) ? 1u : 0u;
-    bounded.push_back(u);
+    chunks.push_back(u);
   }
 }
+
+// First activation slot of each (tables index, pair) for every segment:
+// slots of pair q of tables n start at base[n][q], one row of nact per segment.
+struct ActRows {
+  std::vector<std::vector<int64_t>> base;
+  int64_t total = 0;
+  ActRows(const std::vector<const ngap_tables*>& ts, int64_t nseg) {
+    for (const ngap_tables* t : ts) {
+      base.emplace_back();
+      for (int32_t nact : t->pair_nact) {
+        base.back().push_back(total);
+        total += (int64_t)nact * nseg;
+      }
+    }
+  }
+  int64_t row(int n, const TileHost& th, int64_t seg) const {
+    return th.pair < 0 ? -1 : base[n][th.pair] + seg * th.nact;
+  }
+};
 
 // Units (already grouped by tile) -> CTA tasks: the long units of cyclic tiles
 // first, one per warp of a task; chunks after them in tasks sized to give
 // every CTA several tasks.
-void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& unbounded,
-                const std::vector<UnitDev>& bounded, int grid, std::vector<TaskDev>& tasks) {
+void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
+                const std::vector<UnitDev>& unbounded, const std::vector<UnitDev>& bounded,
+                int grid, std::vector<TaskDev>& tasks, int32_t* ntasks1) {
   units.clear();
   tasks.clear();
+  units.insert(units.end(), pass1.begin(), pass1.end());
+  const size_t np1 = units.size();
   units.insert(units.end(), unbounded.begin(), unbounded.end());
   const size_t nunb = units.size();
   units.insert(units.end(), bounded.begin(), bounded.end());
-  const int64_t per_b = std::max<int64_t>(
-      kWarpsPerCta, std::min<int64_t>(512, (int64_t)bounded.size() / std::max(1, 4 * grid)));
+  auto per = [&](size_t n) {
+    return std::max<int64_t>(kWarpsPerCta,
+                             std::min<int64_t>(512, (int64_t)n / std::max(1, 4 * grid)));
+  };
   auto cut = [&](size_t b, size_t e, int64_t per) {
     size_t i = b;
     while (i < e) {
@@ -426,21 +491,61 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& unbound
       i = j;
     }
   };
-  cut(0, nunb, kWarpsPerCta);
-  cut(nunb, units.size(), per_b);
+  cut(0, np1, per(pass1.size()));
+  *ntasks1 = (int32_t)tasks.size();
+  cut(np1, nunb, kWarpsPerCta);
+  cut(nunb, units.size(), per(bounded.size()));
 }
 
 void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vector<UnitDev>& units,
-                std::vector<TaskDev>& tasks) {
-  std::vector<UnitDev> unbounded, bounded;
+                std::vector<TaskDev>& tasks, int32_t* ntasks1, int64_t* act_entries) {
+  std::vector<UnitDev> pass1, unbounded, bounded;
+  const ActRows rows({t}, k.num_seg);
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
     for (int64_t s = 0; s < k.num_seg; s++) {
       SegSpec sp{s * k.seg_len, (s + 1) * k.seg_len, k.first_seg + s == 0 || k.is_dup != 0, 0ull,
                  0};
-      add_units(t->tiles[ti], ti, sp, k.window, k.chunk, unbounded, bounded);
+      add_units(t->tiles[ti], ti, sp, k.window, k.chunk, rows.row(0, t->tiles[ti], s), pass1,
+                unbounded, bounded);
     }
   }
-  make_tasks(units, unbounded, bounded, grid, tasks);
+  make_tasks(units, pass1, unbounded, bounded, grid, tasks, ntasks1);
+  *act_entries = rows.total;
+}
+
+// Activation slots for the plan, all set to "no match yet".
+int ensure_act(ngap_engine* e) {
+  if (e->act_entries > e->act_cap) {
+    cudaFree(e->d_act);
+    e->d_act = nullptr;
+    e->act_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_act, (size_t)e->act_entries * sizeof(uint32_t)));
+    e->act_cap = e->act_entries;
+  }
+  return NGAP_OK;
+}
+
+// The matching launches of a plan: the activation tiles' tasks, then the rest
+// (the layered tiles read what the first launch recorded).
+template <int PRIV>
+int launch_plan(ngap_engine* e, MatchParams mp, int smem, cudaStream_t st) {
+  if (e->act_entries > 0)
+    CUDA_TRY(cudaMemsetAsync(e->d_act, 0xff, (size_t)e->act_entries * sizeof(uint32_t), st));
+  if (e->ntasks1 > 0) {
+    mp.ntasks = e->ntasks1;
+    match_kernel<PRIV><<<std::max(1, std::min(e->grid, e->ntasks1)), kCtaThreads, smem, st>>>(mp);
+    CUDA_TRY(cudaGetLastError());
+    e->launches++;
+    CUDA_TRY(cudaMemsetAsync(mp.task_counter, 0, sizeof(unsigned int), st));
+  }
+  if (e->ntasks > e->ntasks1) {
+    mp.tasks = e->d_tasks + e->ntasks1;
+    mp.ntasks = e->ntasks - e->ntasks1;
+    match_kernel<PRIV><<<std::max(1, std::min(e->grid, mp.ntasks)), kCtaThreads, smem, st>>>(mp);
+    CUDA_TRY(cudaGetLastError());
+    e->launches++;
+  }
+  return NGAP_OK;
 }
 
 __global__ void swap_halves(uint64_t* a, uint64_t n) {
@@ -473,13 +578,6 @@ int blocks_per_sm(int smem, int* out) {
     set_error("the matching kernel does not fit on an SM with %d bytes of shared memory", smem);
     return NGAP_E_CUDA;
   }
-  return NGAP_OK;
-}
-
-template <int PRIV>
-int launch_match(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t st) {
-  match_kernel<PRIV><<<e->grid, kCtaThreads, smem, st>>>(mp);
-  CUDA_TRY(cudaGetLastError());
   return NGAP_OK;
 }
 
@@ -752,10 +850,14 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   const int full_grid = e->num_sms * bps;
   // units and tasks
   UnitPlanKey key{p->num_seg, p->seg_len, p->is_dup ? 1 : 0, window, p->chunk, p->first_segment};
-  if (e->plan_tables != t || key < e->plan_key || e->plan_key < key) {
+  if (e->plan_tables != t->serial || key < e->plan_key || e->plan_key < key) {
     std::vector<UnitDev> units;
     std::vector<TaskDev> tasks;
-    plan_units(t, key, full_grid, units, tasks);
+    int32_t ntasks1 = 0;
+    int64_t act_entries = 0;
+    plan_units(t, key, full_grid, units, tasks, &ntasks1, &act_entries);
+    e->ntasks1 = ntasks1;
+    e->act_entries = act_entries;
     if (units.size() > e->units_cap) {
       cudaFree(e->d_units);
       e->d_units = nullptr;
@@ -778,14 +880,15 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
                           cudaMemcpyHostToDevice));
     e->nunits = (int32_t)units.size();
     e->ntasks = (int32_t)tasks.size();
-    e->plan_tables = t;
+    e->plan_tables = t->serial;
     e->plan_key = key;
-    e->batch_ts = nullptr;  // the batched plan cache no longer describes the buffers
+    e->batch_ts = 0;  // the batched plan cache no longer describes the buffers
   }
   const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
-  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states);
+  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states, t->max_nact);
   if (rc != NGAP_OK) return rc;
+  if ((rc = ensure_act(e)) != NGAP_OK) return rc;
 
   CUDA_TRY(cudaEventRecord(e->ev[0], st));
   if (input_on_device)
@@ -821,13 +924,15 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.mark_words = e->mark_words;
   mp.ovf_cap = e->ovf_cap;
   mp.work = e->d_counters + 2;
+  mp.act = e->d_act;
+  mp.stk_g = e->d_stk;
+  mp.stk_g_cap = e->stk_cap;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
   if (e->ntasks > 0) {
-    if (priv == 0) rc = launch_match<0>(e, mp, smem, st);
-    else if (priv == 1) rc = launch_match<1>(e, mp, smem, st);
-    else rc = launch_match<2>(e, mp, smem, st);
+    if (priv == 0) rc = launch_plan<0>(e, mp, smem, st);
+    else if (priv == 1) rc = launch_plan<1>(e, mp, smem, st);
+    else rc = launch_plan<2>(e, mp, smem, st);
     if (rc != NGAP_OK) return rc;
-    e->launches++;
   }
   CUDA_TRY(cudaEventRecord(e->ev[2], st));
   if (!p->report_off) {
@@ -949,10 +1054,12 @@ int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, u
 // ---------------------------------------------------------------------------
 
 struct ngap_tableset {
+  uint64_t serial = g_next_serial.fetch_add(1);
   std::vector<const ngap_tables*> tables;
   std::vector<int> tile_base;  // first tile of each NFA in the combined descriptor array
   TileDev* d_tiles = nullptr;
   int ntiles = 0, image_region = 0, max_states = 0, max_groups = 1, max_depth = 1, device = 0;
+  int max_nact = 0;
   ~ngap_tableset() { cudaFree(d_tiles); }
 };
 
@@ -978,6 +1085,7 @@ int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset*
     ts->image_region = std::max(ts->image_region, t->image_region);
     ts->max_states = std::max(ts->max_states, t->max_states);
     ts->max_groups = std::max(ts->max_groups, t->num_groups);
+    ts->max_nact = std::max(ts->max_nact, t->max_nact);
     for (auto& th : t->tiles) ts->max_depth = std::max(ts->max_depth, th.depth);
   }
   ts->device = tables[0]->device;
@@ -1068,12 +1176,13 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     return true;
   };
   bool replanned = false;
-  if (e->batch_ts != ts || e->batch_window != window || e->batch_chunk != p->chunk ||
-      !same_streams() || e->plan_tables != nullptr) {
+  if (e->batch_ts != ts->serial || e->batch_window != window || e->batch_chunk != p->chunk ||
+      !same_streams() || e->plan_tables != 0) {
     std::vector<std::vector<int>> by_nfa(ts->tables.size());
     for (int i = 0; i < nstreams; i++) by_nfa[sv[i].nfa].push_back(i);
-    std::vector<UnitDev> unbounded, bounded, units;
+    std::vector<UnitDev> pass1, unbounded, bounded, units;
     std::vector<TaskDev> tasks;
+    const ActRows rows(ts->tables, nstreams);
     for (size_t n = 0; n < ts->tables.size(); n++) {
       const ngap_tables* t = ts->tables[n];
       for (int ti = 0; ti < (int)t->tiles.size(); ti++)
@@ -1082,10 +1191,12 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
           if (s.length == 0) continue;
           SegSpec sp{(int64_t)s.offset, (int64_t)(s.offset + s.length), true,
                      (uint64_t)si << sshift, (int64_t)s.offset};
-          add_units(t->tiles[ti], ts->tile_base[n] + ti, sp, window, p->chunk, unbounded, bounded);
+          add_units(t->tiles[ti], ts->tile_base[n] + ti, sp, window, p->chunk,
+                    rows.row((int)n, t->tiles[ti], si), pass1, unbounded, bounded);
         }
     }
-    make_tasks(units, unbounded, bounded, full_grid, tasks);
+    make_tasks(units, pass1, unbounded, bounded, full_grid, tasks, &e->ntasks1);
+    e->act_entries = rows.total;
     if (units.size() > e->units_cap) {
       cudaFree(e->d_units);
       e->d_units = nullptr;
@@ -1108,9 +1219,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
                           cudaMemcpyHostToDevice));
     e->nunits = (int32_t)units.size();
     e->ntasks = (int32_t)tasks.size();
-    e->plan_tables = nullptr;  // the plain plan cache no longer describes the buffers
+    e->plan_tables = 0;  // the plain plan cache no longer describes the buffers
     e->plan_key = UnitPlanKey{-1, -1, -1, -1, -1, -1};
-    e->batch_ts = ts;
+    e->batch_ts = ts->serial;
     e->batch_streams = sv;
     e->batch_window = window;
     e->batch_chunk = p->chunk;
@@ -1118,7 +1229,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   }
   const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
-  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states)) != NGAP_OK) return rc;
+  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states, ts->max_nact)) != NGAP_OK)
+    return rc;
+  if ((rc = ensure_act(e)) != NGAP_OK) return rc;
 
   MatchParams mp;
   mp.tiles = ts->d_tiles;
@@ -1145,6 +1258,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   mp.mark_words = e->mark_words;
   mp.ovf_cap = e->ovf_cap;
   mp.work = e->d_counters + 2;
+  mp.act = e->d_act;
+  mp.stk_g = e->d_stk;
+  mp.stk_g_cap = e->stk_cap;
 
   auto enqueue = [&](cudaStream_t qs) -> int {
     if (input_on_device)
@@ -1156,10 +1272,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, sizeof(unsigned int), qs));
     int r = NGAP_OK;
     if (e->ntasks > 0) {
-      r = priv == 0 ? launch_match<0>(e, mp, smem, qs)
-                    : priv == 1 ? launch_match<1>(e, mp, smem, qs) : launch_match<2>(e, mp, smem, qs);
+      r = priv == 0 ? launch_plan<0>(e, mp, smem, qs)
+                    : priv == 1 ? launch_plan<1>(e, mp, smem, qs) : launch_plan<2>(e, mp, smem, qs);
       if (r != NGAP_OK) return r;
-      e->launches++;
     }
     if (!p->report_off) {
       r = sort_unique_fields(e, e->d_counters + 0, cap, ibits, oshift, obits, sshift, sbits,
@@ -1196,7 +1311,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     CUDA_TRY(cudaEventCreateWithFlags(&e->cap_ev[1], cudaEventDisableTiming));
   }
   cudaStream_t cs = e->cap_stream;
-  std::vector<uint64_t> key = {(uint64_t)(uintptr_t)ts, (uint64_t)(uintptr_t)input, input_bytes,
+  std::vector<uint64_t> key = {ts->serial, (uint64_t)(uintptr_t)input, input_bytes,
                                (uint64_t)input_on_device, (uint64_t)p->algorithm,
                                (uint64_t)p->unique, (uint64_t)p->active_threshold,
                                (uint64_t)p->report_off, cap, (uint64_t)window, (uint64_t)p->chunk};

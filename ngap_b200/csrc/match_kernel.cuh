@@ -76,7 +76,13 @@ struct MatchParams {
   uint32_t* ovf;            // [slots][ovf_cap]
   int32_t carry_cap, mark_words, ovf_cap;
   unsigned long long* work; // [0] entries expanded, [1] entries injected
+  uint32_t* act;            // activation slots (first match of sticky states, offset in the
+                            // segment; 0xffffffff = none)
+  uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
+  int32_t stk_g_cap;        // kStickyCap
 };
+
+constexpr uint32_t kNoAct = 0xffffffffu;
 
 // A window buffer: up to kMaxDepth - 1 look-behind bytes, 15 bytes of
 // alignment, W window bytes and one look-ahead byte.
@@ -117,6 +123,8 @@ struct WarpRun {
   uint32_t* ovf;
   uint32_t* carry;
   uint32_t* marks;
+  uint32_t* act;   // activation units: the segment's slots (reports become atomicMin)
+  int stk_cap;     // capacity of the sticky list (ws.stk_s / stk_q)
 };
 
 // The tile a warp works on: hot tables in shared memory (or global memory
@@ -235,6 +243,10 @@ __device__ __forceinline__ void flush_reports(const MatchParams& p, WarpSmem& ws
 // Warp-aggregated report emission: lanes with pred append (offset, id).
 __device__ __forceinline__ void emit_report(const MatchParams& p, WarpSmem& ws, WarpRun& w, int lane,
                                             bool pred, uint32_t id, uint32_t off) {
+  if (w.act) {  // activation pass: id is the sticky state's slot
+    if (pred) atomicMin(w.act + id, off - w.base);
+    return;
+  }
   const unsigned m = __ballot_sync(kFull, pred);
   if (m == 0) return;
   const int cnt = __popc(m);
@@ -414,7 +426,7 @@ __device__ __forceinline__ bool register_sticky(const MatchParams& p, WarpSmem& 
     __syncwarp();
     if (lane == 0) ws.stk_q[found] = (uint32_t)q;
   } else {
-    if (w.nstk >= kStickyCap) return false;
+    if (w.nstk >= w.stk_cap) return false;
     if (lane == 0) {
       ws.stk_s[w.nstk] = s;
       ws.stk_q[w.nstk] = (uint32_t)q;
@@ -539,14 +551,18 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
   __syncwarp();
 }
 
+__device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                                 const TileView& tv, const UnitCtx& c, int lane,
+                                                 int r0, int batch);
+
 // Injection of a batch of positions: always-active states, then the sticky
 // states met while copying, then the work of every active sticky state at
-// these positions.
+// these positions. Layered tiles (phase 2) do their sticky work separately.
 __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpRun& w,
                                        const TileView& tv, const UnitCtx& c, int lane, int r0,
                                        int batch, int depth, unsigned long long& n_injected) {
   inject_aas(p, ws, w, tv, c, lane, r0, batch, depth, n_injected);
-  if (!tv.sticky) return;
+  if (!tv.sticky || tv.t->phase == 2) return;
   __syncwarp();
   const int np = min((int)*ws.pend_n, kPendCap);
   for (int i = 0; i < np; i++) {
@@ -559,10 +575,16 @@ __device__ __forceinline__ void inject(const MatchParams& p, WarpSmem& ws, WarpR
   __syncwarp();
   if (lane == 0) *ws.pend_n = 0u;
   __syncwarp();
+  sticky_positions(p, ws, w, tv, c, lane, r0, batch);
+}
+
+// Work of every active sticky state at window offsets [r0, r0 + batch)
+// (lanes over positions): count the successors that match, one prefix sum,
+// write; reports (rare) through the warp-collective path.
+__device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                                 const TileView& tv, const UnitCtx& c, int lane,
+                                                 int r0, int batch) {
   if (w.nstk == 0) return;
-  // every active sticky state at this batch's positions (lanes over positions):
-  // count the successors that match, one prefix sum, write; reports (rare)
-  // through the warp-collective path
   const int r = r0 + lane;
   const bool valid = lane < batch && r < c.wlen;
   const int64_t t = c.wb + r;
@@ -777,6 +799,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   w.ovf = p.ovf + (size_t)slot * p.ovf_cap;
   w.carry = p.carry + (size_t)slot * p.carry_cap;
   w.marks = p.marks + (size_t)slot * p.mark_words;
+  w.act = nullptr;
+  w.stk_cap = kStickyCap;
+  uint32_t* const stk_smem = ws.stk_s;
   if (lane == 0) {
     mbar_init(&ws.bar[0], 1);
     mbar_init(&ws.bar[1], 1);
@@ -846,10 +871,23 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
     const bool translate = t->cw != 8;
-    // Without sticky states, the last depth - 1 positions of a window are
-    // injected at the start of the next one (from look-behind bytes), so that
-    // every position but the unit's last ones gets the full table depth.
-    const int defer = (depth > 1 && !tv.sticky) ? depth - 1 : 0;
+    // Without sticky states registered during the window (plain tiles
+    // without them, layered tiles), the last depth - 1 positions of a window
+    // are injected at the start of the next one (from look-behind bytes), so
+    // that every position but the unit's last ones gets the full table depth.
+    const bool layered = t->phase == 2;
+    const int defer = (depth > 1 && (!tv.sticky || layered)) ? depth - 1 : 0;
+    // sticky list: shared memory, or global memory for layered tiles with
+    // more slots than that holds
+    if (layered && t->nact > kStickyCap && p.stk_g_cap >= t->nact) {
+      ws.stk_s = p.stk_g + (size_t)slot * 2 * p.stk_g_cap;
+      ws.stk_q = ws.stk_s + p.stk_g_cap;
+      w.stk_cap = p.stk_g_cap;
+    } else {
+      ws.stk_s = stk_smem;
+      ws.stk_q = stk_smem + kStickyCap;
+      w.stk_cap = kStickyCap;
+    }
 
     while (!dead) {
       unsigned uid = 0;
@@ -863,6 +901,33 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       w.nstk = 0;  // sticky states are per unit
       w.key_hi = un.key_hi;
       w.base = (uint32_t)un.base;
+      w.act = t->phase == 1 ? p.act + un.act_row : nullptr;
+      if (layered) {
+        // sticky states whose first match (from the activation pass) comes
+        // before the unit's end: active from there on; a reporting one also
+        // reports at its first match
+        for (int i0 = 0; i0 < t->nact; i0 += 32) {
+          const int i = i0 + lane;
+          const uint32_t f = i < t->nact ? p.act[un.act_row + i] : kNoAct;
+          const int64_t q = un.base + (int64_t)f;
+          const bool ok = f != kNoAct && q < c.hi;
+          const unsigned m = __ballot_sync(kFull, ok);
+          const uint32_t sv = ok ? __ldg(t->act_local + i) : 0u;
+          if (ok) {
+            const int k = w.nstk + __popc(m & lanemask_lt(lane));
+            if (k < w.stk_cap) {
+              ws.stk_s[k] = sv;
+              ws.stk_q[k] = (uint32_t)q;
+            } else {
+              atomicOr(p.err, kErrQueue);
+            }
+          }
+          w.nstk = min(w.nstk + __popc(m), w.stk_cap);
+          const bool rep = ok && is_report(tv, sv) && q >= c.emit_lo;
+          emit_report(p, ws, w, lane, rep, rep ? __ldg(t->sid + sv) : 0u, (uint32_t)q);
+        }
+        __syncwarp();
+      }
       int cur = 0;
       uint32_t nbytes[2], skip[2];
       nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
@@ -919,13 +984,22 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         // next window offset to inject: negative for positions deferred from
         // the previous window (at most `defer` of them)
         int cursor = (int)(inj_pos - wb);
+        // layered tiles: next window offset of the sticky states' work
+        int scur = layered && w.nstk > 0 ? 0 : c.wlen;
         while (true) {
           // inject only when the overflow stack is empty, so that it holds at
           // most one batch's excess
-          if (w.top < kInjectLow && w.ovf_n == 0 && cursor < c.iend) {
-            inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
-            cursor += batch;
-            continue;
+          if (w.top < kInjectLow && w.ovf_n == 0) {
+            if (cursor < c.iend) {
+              inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
+              cursor += batch;
+              continue;
+            }
+            if (scur < c.wlen) {
+              sticky_positions(p, ws, w, tv, c, lane, scur, 32);
+              scur += 32;
+              continue;
+            }
           }
           if (w.top == 0) {
             if (w.ovf_n > 0) {  // refill from the overflow stack
@@ -936,7 +1010,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
               __syncwarp();
               continue;
             }
-            if (cursor < c.iend) continue;
+            if (cursor < c.iend || scur < c.wlen) continue;
             break;
           }
           expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);

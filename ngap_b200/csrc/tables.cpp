@@ -43,9 +43,100 @@ namespace {
 struct CcInfo {
   int32_t group;        // group index (report ids carry it in bits 22 and up)
   int32_t begin, end;   // group-local state range
-  bool bounded;
+  bool bounded;         // acyclic once edges into always-active states are dropped
+  bool layered;         // cyclic only through sticky self-loops (see layer_flags)
   int32_t max_path;
 };
+
+// Sticky states of a CC: not always-active, a self-loop, every byte accepted.
+// Such a state, once matched, matches at every later position of the segment.
+void sticky_flags(const GroupGraph& g, int32_t b, int32_t e, std::vector<char>& sticky) {
+  sticky.assign(e - b, 0);
+  for (int32_t v = b; v < e; v++) {
+    if (g.attrs[v] & 1) continue;
+    bool all = true;
+    for (int w = 0; w < 8; w++) all = all && g.bits[(size_t)v * 8 + w] == 0xffffffffu;
+    if (!all) continue;
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++)
+      if (g.cols[k] == v) sticky[v - b] = 1;
+  }
+}
+
+// A CC is layered when it has sticky states, the graph without edges into
+// always-active states and without sticky self-loops is acyclic, and no sticky
+// state is reachable from another one. Then the first match of each sticky
+// state depends only on an acyclic part (its "pre" states: those with a path
+// to a sticky state through non-sticky states), and once the first matches
+// are known the rest is acyclic with the sticky states as sources. Returns
+// false otherwise; on success pre[] marks the pre states (stickies included),
+// and lp1 / lp2 are the longest paths (in states) of the activation part and
+// of the part with the sticky states as sources.
+bool layer_flags(const GroupGraph& g, int32_t b, int32_t e, std::vector<char>& sticky,
+                 std::vector<char>& pre, int32_t& lp1, int32_t& lp2) {
+  const int32_t n = e - b;
+  sticky_flags(g, b, e, sticky);
+  bool any = false;
+  for (char x : sticky) any = any || x;
+  if (!any) return false;
+  auto edge_ok = [&](int32_t v, int32_t u) {  // kept edge v -> u (group ids)
+    return !(g.attrs[u] & 1) && !(u == v && sticky[v - b]);
+  };
+  std::vector<int32_t> indeg(n, 0), order;
+  order.reserve(n);
+  for (int32_t v = b; v < e; v++)
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++)
+      if (edge_ok(v, g.cols[k])) indeg[g.cols[k] - b]++;
+  for (int32_t i = 0; i < n; i++)
+    if (indeg[i] == 0) order.push_back(i);
+  for (size_t h = 0; h < order.size(); h++) {
+    const int32_t v = order[h] + b;
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (edge_ok(v, u) && --indeg[u - b] == 0) order.push_back(u - b);
+    }
+  }
+  if ((int32_t)order.size() != n) return false;
+  // no sticky state reachable from a sticky state
+  std::vector<char> from(n, 0);
+  for (int32_t i : order) {
+    const int32_t v = i + b;
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (edge_ok(v, u) && (sticky[i] || from[i])) from[u - b] = 1;
+    }
+  }
+  for (int32_t i = 0; i < n; i++)
+    if (sticky[i] && from[i]) return false;
+  // pre states, in reverse topological order
+  pre.assign(n, 0);
+  for (int32_t h = n - 1; h >= 0; h--) {
+    const int32_t i = order[h], v = i + b;
+    if (sticky[i]) {
+      pre[i] = 1;
+      continue;
+    }
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (edge_ok(v, u) && pre[u - b]) pre[i] = 1;
+    }
+  }
+  // longest paths: lp1 over pre states (edges out of stickies dropped), lp2
+  // over all states with edges into stickies dropped
+  std::vector<int32_t> d1(n, 1), d2(n, 1);
+  lp1 = lp2 = 0;
+  for (int32_t i : order) {
+    const int32_t v = i + b;
+    lp2 = std::max(lp2, d2[i]);
+    if (pre[i]) lp1 = std::max(lp1, d1[i]);
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (!edge_ok(v, u)) continue;
+      if (!sticky[u - b]) d2[u - b] = std::max(d2[u - b], d2[i] + 1);
+      if (pre[i] && pre[u - b] && !sticky[i]) d1[u - b] = std::max(d1[u - b], d1[i] + 1);
+    }
+  }
+  return true;
+}
 
 // Longest path (in states) of a CC whose edges into always-active states are
 // removed; -1 if a cycle remains.
@@ -318,26 +409,50 @@ int degree_error() {
   return NGAP_E_INVALID;
 }
 
-bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
-               const TableOpts& opts, std::vector<TileHost>& tiles) {
+// Tile variants: kPlain (the CCs as they are), kActivation (layered CCs: their
+// pre states, sticky states terminal and reported as activations into slots
+// 0..nact-1), kLayered (layered CCs without edges into sticky states, the
+// sticky states pre-registered from the activation pass).
+enum { kPlain = 0, kActivation = 1, kLayered = 2 };
+
+bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, int variant,
+               int pair, const TableOpts& opts, std::vector<TileHost>& tiles) {
   if (ccs.empty()) return true;
   TileHost t;
   t.group = ccs[0].group;
+  t.phase = variant;
+  t.pair = variant == kPlain ? -1 : pair;
+  // per CC: local ids of its states in the tile (-1: not in the tile) and sticky flags
+  std::vector<std::vector<int32_t>> loc(ccs.size());
+  std::vector<std::vector<char>> stk(ccs.size());
   int32_t n = 0;
   bool bounded = true;
   int32_t mp = 0;
   Partition part;
-  for (auto& c : ccs) {
+  for (size_t ci = 0; ci < ccs.size(); ci++) {
+    const CcInfo& c = ccs[ci];
     const GroupGraph& g = gs.groups[c.group];
-    n += c.end - c.begin;
-    bounded = bounded && c.bounded;
-    mp = std::max(mp, c.max_path);
-    for (int32_t v = c.begin; v < c.end; v++) part.refine(&g.bits[(size_t)v * 8]);
+    std::vector<char> pre;
+    int32_t lp1 = 0, lp2 = 0;
+    if (variant != kPlain) {
+      if (!layer_flags(g, c.begin, c.end, stk[ci], pre, lp1, lp2)) return false;
+      mp = std::max(mp, variant == kActivation ? lp1 : lp2);
+    } else {
+      bounded = bounded && c.bounded;
+      mp = std::max(mp, c.max_path);
+    }
+    loc[ci].assign(c.end - c.begin, -1);
+    for (int32_t v = c.begin; v < c.end; v++) {
+      if (variant == kActivation && !pre[v - c.begin]) continue;
+      loc[ci][v - c.begin] = n++;
+      part.refine(&g.bits[(size_t)v * 8]);
+    }
   }
   t.nstates = n;
   t.num_ccs = (int32_t)ccs.size();
   t.max_path = bounded ? mp : -1;
   t.global = global;
+  if (n == 0) return true;
   t.cw = class_words(part.n);
   t.cls.resize(256);
   if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
@@ -347,10 +462,12 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
   } else {
     // bytes no state accepts share one (dead) class; number it last
     uint32_t any[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (auto& c : ccs) {
+    for (size_t ci = 0; ci < ccs.size(); ci++) {
+      const CcInfo& c = ccs[ci];
       const GroupGraph& g = gs.groups[c.group];
       for (int32_t v = c.begin; v < c.end; v++)
-        for (int w = 0; w < 8; w++) any[w] |= g.bits[(size_t)v * 8 + w];
+        if (loc[ci][v - c.begin] >= 0)
+          for (int w = 0; w < 8; w++) any[w] |= g.bits[(size_t)v * 8 + w];
     }
     int dead = -1;
     for (int b = 0; b < 256 && dead < 0; b++)
@@ -369,11 +486,15 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
   t.rep.assign((n + 31) / 32, 0);
   t.sid.resize(n);
   std::vector<uint32_t> aas_bit((n + 31) / 32, 0);
-  int32_t local = 0;
-  for (auto& c : ccs) {
+  t.sticky.assign((n + 31) / 32, 0);
+  for (size_t ci = 0; ci < ccs.size(); ci++) {
+    const CcInfo& c = ccs[ci];
     const GroupGraph& g = gs.groups[c.group];
-    const int32_t first = local;  // local id of the CC's first state
-    for (int32_t v = c.begin; v < c.end; v++, local++) {
+    const std::vector<int32_t>& lc = loc[ci];
+    for (int32_t v = c.begin; v < c.end; v++) {
+      const int32_t local = lc[v - c.begin];
+      if (local < 0) continue;
+      const bool sv = variant != kPlain && stk[ci][v - c.begin];
       t.sid[local] = (uint32_t)v | ((uint32_t)c.group << 22);
       const uint32_t* bv = &g.bits[(size_t)v * 8];
       for (int w = 0; w < 8; w++) t.bits[(size_t)local * 8 + w] = bv[w];
@@ -382,7 +503,20 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
           int cl = t.cls[b];
           t.cmask[(size_t)local * t.cw + (cl >> 5)] |= 1u << (cl & 31);
         }
-      if (g.attrs[v] & 2) t.rep[local >> 5] |= 1u << (local & 31);
+      if (variant == kActivation) {
+        // sticky states are the only reports; their id is the activation slot
+        if (sv) {
+          t.rep[local >> 5] |= 1u << (local & 31);
+          t.sid[local] = (uint32_t)t.nact++;
+        }
+      } else if (g.attrs[v] & 2) {
+        t.rep[local >> 5] |= 1u << (local & 31);
+      }
+      if (variant == kLayered && sv) {
+        t.sticky[local >> 5] |= 1u << (local & 31);
+        t.act_local.push_back((uint32_t)local);
+        t.nact++;
+      }
       if (g.attrs[v] & 1) {
         t.aas.push_back((uint32_t)local);
         aas_bit[local >> 5] |= 1u << (local & 31);
@@ -391,30 +525,40 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
       for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
         int32_t u = g.cols[k];
         if (g.attrs[u] & 1) continue;  // redundant: u is active at every position
+        if (variant == kActivation && sv) continue;  // sticky states end the activation part
+        if (variant != kPlain && stk[ci][u - c.begin]) {
+          // into a sticky state: kept only by the activation part (not its self-loop)
+          if (variant == kLayered || u == v) continue;
+        }
+        const int32_t ul = lc[u - c.begin];
+        if (ul < 0) continue;          // not a pre state: no path to a sticky state
         if (j >= 4) return false;      // the degree limiter guarantees at most 4
-        uint32_t ul = (uint32_t)(first + (u - c.begin));
-        t.succ[(size_t)local * 4 + j++] = ul | ((g.attrs[u] & 2) ? 0x80000000u : 0u);
+        const bool urep = variant == kActivation ? (bool)stk[ci][u - c.begin]
+                                                 : (g.attrs[u] & 2) != 0;
+        t.succ[(size_t)local * 4 + j++] = (uint32_t)ul | (urep ? 0x80000000u : 0u);
       }
     }
     // start-of-data states of the CC, ascending (the group's list is ascending)
     auto lo = std::lower_bound(g.starts.begin(), g.starts.end(), c.begin);
     for (auto it = lo; it != g.starts.end() && *it < c.end; ++it)
-      t.start.push_back((uint32_t)(first + (*it - c.begin)));
+      if (lc[*it - c.begin] >= 0) t.start.push_back((uint32_t)lc[*it - c.begin]);
   }
-  // sticky states: not always-active, a self-loop and every byte accepted; once
-  // such a state matches it matches at every later position of the segment
-  t.sticky.assign((n + 31) / 32, 0);
-  for (int32_t v = 0; v < n; v++) {
-    bool all = true;
-    for (int w = 0; w < 8; w++) all = all && t.bits[(size_t)v * 8 + w] == 0xffffffffu;
-    bool self = false;
-    for (int j = 0; j < 4; j++) self = self || (t.succ[(size_t)v * 4 + j] & 0x7fffffffu) == (uint32_t)v;
-    const bool aas = (aas_bit[v >> 5] >> (v & 31)) & 1u;
-    if (all && self && !aas) {
-      t.sticky[v >> 5] |= 1u << (v & 31);
-      t.nsticky++;
+  // sticky states of plain tiles: not always-active, a self-loop and every
+  // byte accepted; once such a state matches it matches at every later
+  // position of the segment (layered tiles marked theirs above; activation
+  // tiles have none: their sticky states are terminal)
+  if (variant == kPlain) {
+    for (int32_t v = 0; v < n; v++) {
+      bool all = true;
+      for (int w = 0; w < 8; w++) all = all && t.bits[(size_t)v * 8 + w] == 0xffffffffu;
+      bool self = false;
+      for (int j = 0; j < 4; j++)
+        self = self || (t.succ[(size_t)v * 4 + j] & 0x7fffffffu) == (uint32_t)v;
+      const bool aas = (aas_bit[v >> 5] >> (v & 31)) & 1u;
+      if (all && self && !aas) t.sticky[v >> 5] |= 1u << (v & 31);
     }
   }
+  for (uint32_t w : t.sticky) t.nsticky += __builtin_popcount(w);
   build_prefix_tables(t, opts, global);
   build_image(t);
   tiles.push_back(std::move(t));
@@ -422,12 +566,14 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global,
 }
 
 // Packs CCs into tiles in order: a tile is closed when the next CC would pass
-// `max_states` or, for shared-memory tiles, the image budget.
+// `max_states` or, for shared-memory tiles, the image budget. Layered CCs are
+// packed into pairs of tiles (activation, layered) over the same CCs.
 class TilePacker {
  public:
-  TilePacker(const GroupSet& gs, const TableOpts& opts, bool global, int64_t max_states,
-             std::vector<TileHost>& tiles)
-      : gs_(gs), opts_(opts), global_(global), max_states_(max_states), tiles_(tiles) {}
+  TilePacker(const GroupSet& gs, const TableOpts& opts, bool global, bool layered,
+             int64_t max_states, int* pairs, std::vector<TileHost>& tiles)
+      : gs_(gs), opts_(opts), global_(global), layered_(layered), max_states_(max_states),
+        pairs_(pairs), tiles_(tiles) {}
 
   bool add(const CcInfo& ci) {
     const GroupGraph& g = gs_.groups[ci.group];
@@ -450,7 +596,16 @@ class TilePacker {
   }
 
   bool flush() {
-    const bool ok = emit_tile(gs_, open_, global_, opts_, tiles_);
+    bool ok = true;
+    if (!open_.empty()) {
+      if (layered_) {
+        const int pair = (*pairs_)++;
+        ok = emit_tile(gs_, open_, global_, kActivation, pair, opts_, tiles_) &&
+             emit_tile(gs_, open_, global_, kLayered, pair, opts_, tiles_);
+      } else {
+        ok = emit_tile(gs_, open_, global_, kPlain, -1, opts_, tiles_);
+      }
+    }
     open_.clear();
     n_ = 0;
     part_ = Partition();
@@ -460,21 +615,66 @@ class TilePacker {
  private:
   const GroupSet& gs_;
   const TableOpts& opts_;
-  bool global_;
+  bool global_, layered_;
   int64_t max_states_;
+  int* pairs_;
   std::vector<TileHost>& tiles_;
   std::vector<CcInfo> open_;
   int64_t n_ = 0;
   Partition part_;
 };
 
+// CC indices of one kind -> the sets that become global tiles. Clusters by
+// alphabet (the bytes any state of the CC accepts) with at most 32 byte
+// classes become global when they would need more than two shared-memory
+// tiles; the remaining CCs of the kind form one more global set when they too
+// would need more than two.
+std::vector<std::vector<int>> global_sets_of(const GroupSet& gs, const std::vector<CcInfo>& ccs,
+                                             const std::vector<int>& kind, const TableOpts& opts) {
+  std::map<std::array<uint32_t, 8>, std::vector<int>> clusters;
+  for (int i : kind) {
+    const GroupGraph& g = gs.groups[ccs[i].group];
+    std::array<uint32_t, 8> alpha{};
+    for (int32_t v = ccs[i].begin; v < ccs[i].end; v++)
+      for (int w = 0; w < 8; w++) alpha[w] |= g.bits[(size_t)v * 8 + w];
+    clusters[alpha].push_back(i);
+  }
+  const int64_t two_tiles = 2 * (int64_t)opts.image_budget;
+  std::vector<std::vector<int>> sets;
+  std::vector<int> rest;
+  Partition rest_part;
+  int64_t rest_n = 0;
+  for (auto& kv : clusters) {
+    Partition part;
+    int64_t n = 0;
+    for (int i : kv.second) {
+      const GroupGraph& g = gs.groups[ccs[i].group];
+      n += ccs[i].end - ccs[i].begin;
+      for (int32_t v = ccs[i].begin; v < ccs[i].end; v++) part.refine(&g.bits[(size_t)v * 8]);
+    }
+    if (class_words(part.n) == 1 && image_bytes(n, 1) > two_tiles) {
+      sets.push_back(kv.second);
+    } else {
+      for (int i : kv.second) {
+        const GroupGraph& g = gs.groups[ccs[i].group];
+        for (int32_t v = ccs[i].begin; v < ccs[i].end; v++) rest_part.refine(&g.bits[(size_t)v * 8]);
+      }
+      rest.insert(rest.end(), kv.second.begin(), kv.second.end());
+      rest_n += n;
+    }
+  }
+  if (!rest.empty() && image_bytes(rest_n, class_words(rest_part.n)) > two_tiles)
+    sets.push_back(rest);
+  return sets;
+}
+
 }  // namespace
 
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles) {
   tiles.clear();
   std::vector<CcInfo> ccs;
-  // acyclic CCs clustered by alphabet (the bytes any of their states accepts)
-  std::map<std::array<uint32_t, 8>, std::vector<int>> clusters;
+  std::vector<int> bounded, layered;
+  std::vector<char> sticky, pre;
   for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
     const GroupGraph& g = gs.groups[gi];
     const int nccs = (int)g.cc_begin.size() - 1;
@@ -486,60 +686,56 @@ int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>
       int32_t lp = cc_longest_path(g, ci.begin, ci.end);
       ci.bounded = lp >= 0 && lp <= opts.max_warmup;
       ci.max_path = ci.bounded ? lp : -1;
-      if (ci.bounded) {
-        std::array<uint32_t, 8> alpha{};
-        for (int32_t v = ci.begin; v < ci.end; v++)
-          for (int w = 0; w < 8; w++) alpha[w] |= g.bits[(size_t)v * 8 + w];
-        clusters[alpha].push_back((int)ccs.size());
+      ci.layered = false;
+      if (!ci.bounded && lp < 0 && opts.layered) {
+        int32_t lp1 = 0, lp2 = 0;
+        ci.layered = layer_flags(g, ci.begin, ci.end, sticky, pre, lp1, lp2) &&
+                     lp1 <= opts.max_warmup && lp2 <= opts.max_warmup;
       }
+      if (ci.bounded) bounded.push_back((int)ccs.size());
+      if (ci.layered) layered.push_back((int)ccs.size());
       ccs.push_back(ci);
     }
   }
-  // A cluster of acyclic CCs becomes global tiles when it would need more than
-  // two shared-memory tiles and its bytes fall into at most 32 classes (keys of
-  // deep prefix tables stay small); everything else, cyclic CCs included, uses
-  // shared-memory tiles. NGAP_TILES_GLOBAL takes every acyclic CC global.
+  // Global tiles (tile_mode 2: every acyclic or layered CC; 0: the sets
+  // global_sets_of picks); everything else, other cyclic CCs included, uses
+  // shared-memory tiles of one group.
   std::vector<char> in_global(ccs.size(), 0);
-  std::vector<std::vector<int>> global_sets;
+  std::vector<std::vector<int>> gsets[2];
   if (opts.tile_mode == 2) {
-    global_sets.emplace_back();
-    for (size_t i = 0; i < ccs.size(); i++)
-      if (ccs[i].bounded) global_sets.back().push_back((int)i);
+    if (!bounded.empty()) gsets[0].push_back(bounded);
+    if (!layered.empty()) gsets[1].push_back(layered);
   } else if (opts.tile_mode == 0) {
-    for (auto& kv : clusters) {
-      Partition part;
-      int64_t n = 0;
-      for (int i : kv.second) {
-        const GroupGraph& g = gs.groups[ccs[i].group];
-        n += ccs[i].end - ccs[i].begin;
-        for (int32_t v = ccs[i].begin; v < ccs[i].end; v++) part.refine(&g.bits[(size_t)v * 8]);
-      }
-      if (class_words(part.n) == 1 && image_bytes(n, 1) > 2 * (int64_t)opts.image_budget)
-        global_sets.push_back(kv.second);
-    }
+    gsets[0] = global_sets_of(gs, ccs, bounded, opts);
+    gsets[1] = global_sets_of(gs, ccs, layered, opts);
   }
-  // Acyclic tiles get parallelism from chunks, so they fill the budget. A
-  // cyclic tile is one sequential unit per segment, so those stay small to
-  // give the GPU enough independent units.
-  const int64_t cap_bounded = opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2;
+  // Acyclic and layered tiles get parallelism from chunks, so they fill the
+  // budget. A cyclic tile is one sequential unit per segment, so those stay
+  // small to give the GPU enough independent units.
+  const int64_t cap_chunked = opts.tile_states > 0 ? opts.tile_states : (int64_t)kMaxTileStates - 2;
   const int64_t cap_cyclic = opts.tile_states > 0 ? opts.tile_states : (int64_t)opts.unbounded_tile_states;
-  for (auto& set : global_sets) {
-    std::sort(set.begin(), set.end());  // (group, CC) order
-    TilePacker pk(gs, opts, true, cap_bounded, tiles);
-    for (int i : set) {
-      in_global[i] = 1;
-      if (!pk.add(ccs[i])) return degree_error();
+  int pairs = 0;
+  for (int k = 0; k < 2; k++)
+    for (auto& set : gsets[k]) {
+      std::sort(set.begin(), set.end());  // (group, CC) order
+      TilePacker pk(gs, opts, true, k == 1, cap_chunked, &pairs, tiles);
+      for (int i : set) {
+        in_global[i] = 1;
+        if (!pk.add(ccs[i])) return degree_error();
+      }
+      if (!pk.flush()) return degree_error();
     }
-    if (!pk.flush()) return degree_error();
-  }
   for (int gi = 0; gi < (int)gs.groups.size(); gi++) {
-    TilePacker b(gs, opts, false, cap_bounded, tiles), u(gs, opts, false, cap_cyclic, tiles);
+    TilePacker b(gs, opts, false, false, cap_chunked, &pairs, tiles);
+    TilePacker l(gs, opts, false, true, cap_chunked, &pairs, tiles);
+    TilePacker u(gs, opts, false, false, cap_cyclic, &pairs, tiles);
     for (size_t i = 0; i < ccs.size(); i++) {
       const CcInfo& ci = ccs[i];
       if (ci.group != gi || in_global[i]) continue;
-      if (!(ci.bounded ? b : u).add(ci)) return degree_error();
+      TilePacker& pk = ci.bounded ? b : (ci.layered ? l : u);
+      if (!pk.add(ci)) return degree_error();
     }
-    if (!b.flush() || !u.flush()) return degree_error();
+    if (!b.flush() || !l.flush() || !u.flush()) return degree_error();
   }
   return NGAP_OK;
 }

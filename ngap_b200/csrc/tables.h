@@ -29,6 +29,10 @@ struct TileHost {
   int32_t inj_batch = 32;            // positions injected per worklist refill
   int32_t inj_batch0 = 32;           // the same without prefix tables (AAS scan)
   bool global = false;               // tables read through L2, never staged in shared memory
+  int32_t phase = 0;                 // 0 plain, 1 activation pass, 2 layered (stickies from pass 1)
+  int32_t pair = -1;                 // activation/layered tiles: index of their pair
+  int32_t nact = 0;                  // activation slots (sticky states) of the pair
+  std::vector<uint32_t> act_local;   // layered: local id of the sticky state of each slot
   std::vector<uint8_t> cls;          // 256: byte -> class, live classes first
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
   std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
@@ -53,6 +57,7 @@ struct TableOpts {
   int64_t auto_table_bytes = 12 << 20;  // automatic depth: prefix-table bytes per tile
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
   int tile_mode = 0;                // 0 automatic, 1 shared-memory tiles, 2 global tiles
+  bool layered = true;              // chunk CCs that are cyclic only through sticky self-loops
   int64_t auto_global_table_bytes = 96 << 20;  // automatic depth, global tiles
   int64_t global_table_entries = 32 << 20;     // list entries per table, global tiles
 };

@@ -276,3 +276,80 @@ def test_dense_reports(engine, algo):
                              algorithm=algo)
         assert len(want) > size // 2
         assert np.array_equal(got, want), size
+
+
+@pytest.mark.parametrize("tile_mode", ["shared", "global"])
+def test_layered_many_active(engine, tile_mode):
+    """Dot-star CCs matched in chunks (activation pass, then layered tiles):
+    1-2 byte prefixes activate hundreds of `.*` states early, more than a
+    warp's shared sticky list holds."""
+    anml, data = W.dotstar_set(seed=41, n_patterns=300, lit_lo=1, lit_hi=2, aas_frac=0.0,
+                               input_len=1 << 16, plant_every=1 << 9)
+    for algo in ("nonblockingpcgroups", "nonblockinggroups", "NAPgroups"):
+        for window in (0, 100):
+            got, want = run_both(engine, anml, data, 3, len(data) // 3, group_num=2, depth=-1,
+                                 algorithm=algo, tile_mode=tile_mode, window=window, chunk=1000)
+            assert len(want) > 100
+            assert np.array_equal(got, want), (algo, window)
+
+
+def _two_star(w, p, rng, lo=2, hi=3):
+    """lit .* lit .* lit: a sticky state reachable from another (not layered)."""
+    lits = [rng.integers(97, 101, size=int(rng.integers(lo, hi + 1))) for _ in range(3)]
+    names = []
+    for k, lit in enumerate(lits):
+        for i, c in enumerate(lit):
+            names.append((f"t{p}l{k}c{i}", int(c)))
+    prev = None
+    for k, lit in enumerate(lits):
+        for i, c in enumerate(lit):
+            nm = f"t{p}l{k}c{i}"
+            last = i == len(lit) - 1
+            nxt = ([f"t{p}s{k}", f"t{p}l{k + 1}c0"] if k < 2 else []) if last else [f"t{p}l{k}c{i + 1}"]
+            w.ste(nm, [int(c)], nxt, start="all-input" if (k == 0 and i == 0) else None,
+                  report=(k == 2 and last))
+        if k < 2:
+            w.ste(f"t{p}s{k}", None, [f"t{p}s{k}", f"t{p}l{k + 1}c0"], symbol_set="*")
+
+
+def test_layered_mixed_with_cyclic(engine):
+    """Layered dot-star CCs next to CCs that stay sequential (two `.*` in a
+    row, a reporting `.*`) and plain literals, over several segments."""
+    rng = np.random.default_rng(42)
+    w = W.AnmlWriter()
+    for p in range(12):
+        _two_star(w, p, rng)
+    for p in range(20):  # lit .* lit with a reporting star
+        a = rng.integers(97, 101, size=2)
+        w.ste(f"r{p}a0", [int(a[0])], [f"r{p}a1"], start="all-input")
+        w.ste(f"r{p}a1", [int(a[1])], [f"r{p}s"])
+        w.ste(f"r{p}s", None, [f"r{p}s", f"r{p}b"], symbol_set="*", report=(p % 2 == 0))
+        w.ste(f"r{p}b", [int(rng.integers(97, 101))], [], report=True)
+    for p in range(10):
+        w.ste(f"x{p}", [int(rng.integers(97, 101))], [f"y{p}"], start="all-input")
+        w.ste(f"y{p}", [int(rng.integers(97, 101))], [], report=True)
+    data = rng.integers(97, 102, size=30000).astype(np.uint8)
+    for algo in ("nonblockingpcgroups", "blockinggroups", "nonblockingallgroups"):
+        for tile_mode in ("auto", "global"):
+            got, want = run_both(engine, w.text(), data, 5, 6000, group_num=3, depth=3,
+                                 algorithm=algo, tile_mode=tile_mode, chunk=700)
+            assert len(want) > 100
+            assert np.array_equal(got, want), (algo, tile_mode)
+
+
+def test_plan_cache_after_tables_freed(engine):
+    """Tables created where freed ones were (same address) get their own unit
+    plan: the engine keys its plan cache by a serial number."""
+    import gc
+    anml, data = W.dotstar_set(seed=43, n_patterns=60, input_len=1 << 15, plant_every=1 << 9)
+    nfa = nb.Nfa.from_string(anml)
+    groups = nb.Groups(nfa, group_num=2)
+    want, _ = oracle.match(groups.views(), data, 2, len(data) // 2)
+    for i in range(8):
+        mode = ("shared", "global", "auto")[i % 3]
+        tables = nb.Tables(groups, precompute_depth=(3, -1)[i % 2], tile_mode=mode,
+                           tile_states=(0, 300)[(i // 2) % 2])
+        got = engine.match(tables, data, 2, len(data) // 2)
+        assert np.array_equal(got, want), (i, mode)
+        del tables
+        gc.collect()
