@@ -69,7 +69,7 @@ def profiled_traffic(workload, num_seg):
     with open(p) as f:
         d = json.load(f)
     v = d.get(workload)
-    if v is None or int(v.get("num_seg", -1)) != num_seg:
+    if v is None or int(v.get("num_seg", v.get("streams", -1))) != num_seg:
         return None
     return float(v["dram_bytes_per_launch"])
 
@@ -160,25 +160,240 @@ def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
     from oracle import oracle
     ncores = os.cpu_count() or 1
     views = groups.views()
+    uq = has_sticky(views)  # the reference's --unique where the loop as written does not end
     nseg_total = len(data) // seg_len
     nseg = 1
     t0 = time.time()
-    reps, st = oracle.match(views, data[:seg_len], 1, seg_len, mode=0, nthreads=ncores)
+    reps, st = oracle.match(views, data[:seg_len], 1, seg_len, mode=0, unique=uq, nthreads=ncores)
     dt = time.time() - t0
     # grow the sample to roughly seconds_hint of CPU work
     while dt < seconds_hint / 4 and nseg * 2 <= nseg_total:
         nseg *= 2
         t0 = time.time()
-        reps, st = oracle.match(views, data[:nseg * seg_len], nseg, seg_len, mode=0, nthreads=ncores)
+        reps, st = oracle.match(views, data[:nseg * seg_len], nseg, seg_len, mode=0, unique=uq,
+                                nthreads=ncores)
         dt = time.time() - t0
     units = len(views) * nseg
     return {
         "value": (nseg * seg_len) / dt / 1e6, "unit": "MB/s", "cores": min(ncores, units),
         "kind": "port",
         "sample": f"{nseg} of {nseg_total} segments ({nseg * seg_len} B), {units} (group, segment) "
-                  f"units, {dt:.1f} s",
+                  f"units, {dt:.1f} s" + ("; --unique (.* states)" if uq else ""),
         "stats": st, "sample_bytes": nseg * seg_len, "sample_reports": int(len(reps)),
     }
+
+
+BATCH_DESC = ("16 NFAs of 2k-200k STEs (literal, Hamming, Levenshtein and dot-star generators), "
+              "4096 streams of log-uniform length 1 KiB-4 MiB (about 2 GiB), one launch")
+
+
+def has_sticky(views):
+    """True when some group has a state that is not always-active, accepts
+    every byte and loops on itself (`.*`): the reference CPU loop as written
+    re-adds such a state once per predecessor path and position, so its
+    frontier grows without bound; the reference's --unique option bounds it."""
+    for v in views:
+        ro, co = v.row_offsets, v.col_indices
+        full = np.all(v.symbol_sets.reshape(-1, 8) == 0xffffffff, axis=1)
+        for s in np.nonzero(full & ((v.node_attrs & 1) == 0))[0]:
+            if s in co[ro[s]:ro[s + 1]]:
+                return True
+    return False
+
+
+def cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=15.0, cap=1 << 14,
+                       mode=0, seed=0):
+    """The oracle on a bounded sample of batched streams: a seeded random order
+    of streams, the first `cap` bytes of each, one stream per host thread,
+    until `seconds` have passed. mode 0 is the reference CPU loop as written,
+    with --unique for NFAs with `.*` states (see has_sticky); mode 1 gives the
+    unique-frontier statistics. Returns MB/s, the sample and frontier stats."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle
+    ncores = os.cpu_count() or 1
+    order = np.random.default_rng(seed).permutation(len(offsets))
+    views = [g.views() for g in groups]
+    uniq = [mode == 0 and has_sticky(v) for v in views]
+
+    def one(i):
+        n = int(min(int(lengths[i]), cap))
+        if n == 0:
+            return 0, None
+        k = int(nfa_of[i])
+        seg = data[int(offsets[i]):int(offsets[i]) + n]
+        return n, oracle.match(views[k], seg, 1, n, mode=mode, unique=uniq[k], nthreads=1)[1]
+
+    t0 = time.time()
+    done, nbytes = 0, 0
+    stats = {"matched": 0, "matched_deg": 0, "reports_raw": 0, "frontier": 0}
+    with ThreadPoolExecutor(ncores) as ex:
+        while done < len(order) and time.time() - t0 < seconds:
+            part = order[done:done + ncores]
+            done += len(part)
+            for n, st in ex.map(one, part):
+                nbytes += n
+                for k in stats:
+                    stats[k] += st[k] if st else 0
+    dt = time.time() - t0
+    sample = f"{done} random streams, first {cap} B of each ({nbytes} B), one per thread, {dt:.1f} s"
+    if any(uniq):
+        sample += f"; --unique for the {sum(uniq)} NFAs with .* states"
+    return {"value": nbytes / dt / 1e6, "unit": "MB/s", "cores": min(ncores, done),
+            "kind": "port", "sample": sample, "bytes": nbytes, "stats": stats}
+
+
+def run_batched(args, warmup, rank, world, local_rank):
+    """The batched suite: every stream's reports from one launch per step."""
+    import torch
+    import ngap_b200 as nb
+    from ngap_b200 import autotune, workloads as W
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    nfas, data, offsets, lengths, nfa_of = W.batched_suite(seed=4)
+    groups = [nb.Groups(nb.Nfa.from_string(n["anml"]), group_num=1) for n in nfas]
+    tables = [nb.Tables(g, device=local_rank, precompute_depth=-1) for g in groups]
+    ts = nb.TableSet(tables)
+    eng = nb.Engine(local_rank)
+    best, tuned = autotune.autotune(eng, ts, data, offsets, lengths, nfa_of, frac=0.01)
+    total = int(lengths.sum())
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    d = torch.from_numpy(data).to(f"cuda:{local_rank}")
+    pinned = torch.from_numpy(data).pin_memory()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(warmup):
+        nb.batch_match_async(eng, ts, d, offsets, lengths, nfa_of, stream=sh, **best)
+        eng.sync()
+    raw, uniq = eng.counts()
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    match_ms, launches = [], 0
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            nb.batch_match_async(eng, ts, d, offsets, lengths, nfa_of, stream=sh, **best)
+            evs[i][1].record(stream)
+            eng.sync()
+            match_ms.append(eng.times_ms()[0])
+            launches += eng.launches()
+        barrier()
+    t_ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * total * args.steps / (t_ms / 1e3) / 1e6
+    # end to end: pinned host input copied in, every stream's reports copied out
+    barrier()
+    e2e_ms, d2h = [], 0
+    for i in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        nb.batch_match_async(eng, ts, pinned.numpy(), offsets, lengths, nfa_of, stream=sh, **best)
+        eng.sync()
+        reps, sids = nb.batch_results(eng)
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+        d2h = reps.nbytes + sids.nbytes + 40
+    e2e_total = float(sum(e2e_ms))
+    if dist is not None:
+        tt = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = world * total * args.steps / (e2e_total / 1e3) / 1e6
+    # plain (one match per stream, sequential) against batched on the same streams
+    sub = list(range(min(512, len(offsets))))
+    sub_b = int(sum(int(lengths[i]) for i in sub))
+    plain_ms = 0.0
+    for i in sub:
+        if lengths[i] == 0:
+            continue
+        seg = d[int(offsets[i]):int(offsets[i] + lengths[i])]
+        eng.match_async(tables[int(nfa_of[i])], seg, 1, int(lengths[i]),
+                        algorithm=best["algorithm"], stream=sh)
+        eng.sync()
+        plain_ms += sum(eng.times_ms())
+    nb.batch_match_async(eng, ts, d, offsets[sub], lengths[sub], nfa_of[sub], stream=sh, **best)
+    eng.sync()
+    sub_batched_ms = sum(eng.times_ms())
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        mk = float(np.mean(match_ms))
+        line = {"metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded generators, same shapes as the benchmark config)",
+                "config": {"workload": "batched_suite", "desc": BATCH_DESC, "streams": len(offsets),
+                           "nfas": len(nfas), "input_bytes": total, "params": best,
+                           "autotune": [[p, round(ms, 3)] for p, ms in tuned],
+                           "l2": "inputs larger than L2 (2 GiB)"},
+                "reports": {"raw": raw, "unique": uniq},
+                "gpu_launches": launches,
+                "clocks": clk.summary(),
+                "e2e": {"value": e2e_value, "unit": "MB/s", "h2d_bytes_per_step": total,
+                        "d2h_bytes_per_step": d2h},
+                "plain_vs_batched": {"streams": len(sub), "bytes": sub_b,
+                                     "plain_mbps": sub_b / plain_ms / 1e3,
+                                     "batched_mbps": sub_b / sub_batched_ms / 1e3}}
+        roof = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                "kernel": "match_kernel", "kernel_ms": mk}
+        if not args.no_cpu_baseline:
+            cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of)
+            cb.pop("stats")
+            cb.pop("bytes")
+            line["cpu_baseline"] = cb
+            fr = cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=8.0, mode=1)
+            per = {k: v / max(1, fr["bytes"]) for k, v in fr["stats"].items()}
+            alg = algorithmic_bytes({k: v * total for k, v in per.items()}, total, uniq,
+                                    sum(t.device_bytes for t in tables))
+            roof.update({"achieved": alg / (mk / 1e3) / 1e9, "algorithmic_bytes": alg,
+                         "bytes_per_input_byte": alg / total,
+                         "frontier_sample": fr["sample"]})
+            roof["frac"] = roof["achieved"] / peak
+        roof["traffic"] = profiled_traffic("batched_suite", len(offsets))
+        line["roofline"] = roof
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_batched_reference(args, warmup):
+    """Reference arm of the batched suite: the reference CPU matcher (the
+    oracle's restatement) over bounded samples of the streams, all host threads."""
+    import ngap_b200 as nb
+    from ngap_b200 import workloads as W
+    nfas, data, offsets, lengths, nfa_of = W.batched_suite(seed=4)
+    groups = [nb.Groups(nb.Nfa.from_string(n["anml"]), group_num=1) for n in nfas]
+    per = max(5.0, 60.0 / max(1, args.steps))
+    vals = []
+    for k in range(args.steps):
+        cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=per, seed=k)
+        vals.append(cb["value"])
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": v, "unit": "MB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": "batched_suite", "desc": BATCH_DESC,
+                       "streams": len(offsets), "nfas": len(nfas)},
+            "cpu_baseline": {"value": v, "unit": "MB/s", "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -198,6 +413,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "batched_suite":
+        if args.impl == "reference":
+            if rank == 0:
+                run_batched_reference(args, warmup)
+            return
+        run_batched(args, warmup, rank, world, local_rank)
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -73,6 +73,7 @@ struct TileDev {
   int32_t phase = 0;        // 0 plain; 1 activation pass; 2 layered (sticky states pre-registered)
   int32_t nact = 0;         // activation slots per segment (phase 1 and 2)
   const uint32_t* act_local = nullptr;  // phase 2: [nact] local id of each slot's sticky state
+  const uint32_t* stk_union = nullptr;  // phase 2: [nact][cw] classes any successor accepts
   const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
   const uint32_t* sid = nullptr;    // [nstates] local -> report id (sid | group << 22)
   const uint32_t* aas = nullptr;    // [naas] local ids
@@ -94,6 +95,8 @@ struct UnitDev {
   int64_t base;      // first byte of the unit's stream
   uint64_t key_hi;   // stream index, already shifted into the report key
   int64_t act_row;   // phase 1 and 2 tiles: first activation slot of the unit's segment
+  int32_t act_rowid; // its row (pair, segment) in the compacted activation lists
+  int32_t pad;
 };
 
 // A CTA-level task: consecutive units [ubegin, uend) of one tile.

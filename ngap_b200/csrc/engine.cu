@@ -123,7 +123,13 @@ struct ngap_engine {
   int32_t ntasks1 = 0;       // tasks of activation tiles, launched first
   int64_t act_entries = 0;   // activation slots the plan uses
   uint32_t* d_act = nullptr;
+  uint32_t* d_act_list = nullptr;  // per row: slots with a first match (compacted)
   int64_t act_cap = 0;
+  int32_t act_rows = 0;            // rows of the plan
+  int64_t* d_row_off = nullptr;    // per row: first slot
+  int32_t* d_row_n = nullptr;      // per row: slots
+  uint32_t* d_act_cnt = nullptr;   // per row: matched slots
+  int32_t rows_cap = 0;
   uint32_t* d_stk = nullptr; // per-slot sticky lists of layered units (beyond shared memory)
   int stk_cap = 0;
   // reports
@@ -186,6 +192,10 @@ struct ngap_engine {
     cudaFree(d_marks);
     cudaFree(d_ovf);
     cudaFree(d_act);
+    cudaFree(d_act_list);
+    cudaFree(d_row_off);
+    cudaFree(d_row_n);
+    cudaFree(d_act_cnt);
     cudaFree(d_stk);
     cudaFree(d_stream_ids);
     if (graph) cudaGraphExecDestroy(graph);
@@ -265,6 +275,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       t->max_nact = std::max(t->max_nact, th.nact);
     }
     if ((rc = t->upload(th.act_local, &d.act_local)) != NGAP_OK) return rc;
+    if ((rc = t->upload(th.stk_union, &d.stk_union)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.image, &d.image)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.sid, &d.sid)) != NGAP_OK) return rc;
     if ((rc = t->upload(th.aas, &d.aas)) != NGAP_OK) return rc;
@@ -409,13 +420,14 @@ struct SegSpec {
 };
 
 void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int chunk_opt,
-               int64_t act_row, std::vector<UnitDev>& pass1, std::vector<UnitDev>& unbounded,
-               std::vector<UnitDev>& bounded) {
+               std::pair<int64_t, int32_t> act, std::vector<UnitDev>& pass1,
+               std::vector<UnitDev>& unbounded, std::vector<UnitDev>& bounded) {
   UnitDev u{};
   u.tile = tile;
   u.key_hi = s.key_hi;
   u.base = s.base;
-  u.act_row = act_row;
+  u.act_row = act.first;
+  u.act_rowid = act.second;
   std::vector<UnitDev>& chunks = th.phase == 1 ? pass1 : bounded;
   const bool starts = s.starts && !th.start.empty();
   if (th.max_path < 0) {
@@ -441,22 +453,33 @@ void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int c
   }
 }
 
-// First activation slot of each (tables index, pair) for every segment:
-// slots of pair q of tables n start at base[n][q], one row of nact per segment.
+// Activation rows: one per (tables index, pair, segment), nact slots each;
+// the slots of pair q of tables n start at base[n][q], its rows at rbase[n][q].
 struct ActRows {
   std::vector<std::vector<int64_t>> base;
+  std::vector<std::vector<int32_t>> rbase;
+  std::vector<int64_t> row_off;  // per row: first slot
+  std::vector<int32_t> row_n;    // per row: slots
   int64_t total = 0;
   ActRows(const std::vector<const ngap_tables*>& ts, int64_t nseg) {
     for (const ngap_tables* t : ts) {
       base.emplace_back();
+      rbase.emplace_back();
       for (int32_t nact : t->pair_nact) {
         base.back().push_back(total);
+        rbase.back().push_back((int32_t)row_off.size());
+        for (int64_t g = 0; g < nseg; g++) {
+          row_off.push_back(total + g * nact);
+          row_n.push_back(nact);
+        }
         total += (int64_t)nact * nseg;
       }
     }
   }
-  int64_t row(int n, const TileHost& th, int64_t seg) const {
-    return th.pair < 0 ? -1 : base[n][th.pair] + seg * th.nact;
+  // (first slot, row id) of a unit of tile th over segment seg; (-1, -1) for plain tiles
+  std::pair<int64_t, int32_t> row(int n, const TileHost& th, int64_t seg) const {
+    if (th.pair < 0) return {-1, -1};
+    return {base[n][th.pair] + seg * th.nact, rbase[n][th.pair] + (int32_t)seg};
   }
 };
 
@@ -497,10 +520,10 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
   cut(nunb, units.size(), per(bounded.size()));
 }
 
-void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vector<UnitDev>& units,
-                std::vector<TaskDev>& tasks, int32_t* ntasks1, int64_t* act_entries) {
+ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
+                   std::vector<UnitDev>& units, std::vector<TaskDev>& tasks, int32_t* ntasks1) {
   std::vector<UnitDev> pass1, unbounded, bounded;
-  const ActRows rows({t}, k.num_seg);
+  ActRows rows({t}, k.num_seg);
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
     for (int64_t s = 0; s < k.num_seg; s++) {
       SegSpec sp{s * k.seg_len, (s + 1) * k.seg_len, k.first_seg + s == 0 || k.is_dup != 0, 0ull,
@@ -510,19 +533,62 @@ void plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid, std::vecto
     }
   }
   make_tasks(units, pass1, unbounded, bounded, grid, tasks, ntasks1);
-  *act_entries = rows.total;
+  return rows;
 }
 
-// Activation slots for the plan, all set to "no match yet".
-int ensure_act(ngap_engine* e) {
+// Activation buffers of a plan (slots, compacted lists, row table).
+int set_act_rows(ngap_engine* e, const ActRows& rows) {
+  e->act_entries = rows.total;
+  e->act_rows = (int32_t)rows.row_off.size();
   if (e->act_entries > e->act_cap) {
     cudaFree(e->d_act);
-    e->d_act = nullptr;
+    cudaFree(e->d_act_list);
+    e->d_act = e->d_act_list = nullptr;
     e->act_cap = 0;
     CUDA_TRY(cudaMalloc(&e->d_act, (size_t)e->act_entries * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&e->d_act_list, (size_t)e->act_entries * sizeof(uint32_t)));
     e->act_cap = e->act_entries;
   }
+  if (e->act_rows > e->rows_cap) {
+    cudaFree(e->d_row_off);
+    cudaFree(e->d_row_n);
+    cudaFree(e->d_act_cnt);
+    e->d_row_off = nullptr;
+    e->d_row_n = nullptr;
+    e->d_act_cnt = nullptr;
+    e->rows_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_row_off, (size_t)e->act_rows * sizeof(int64_t)));
+    CUDA_TRY(cudaMalloc(&e->d_row_n, (size_t)e->act_rows * sizeof(int32_t)));
+    CUDA_TRY(cudaMalloc(&e->d_act_cnt, (size_t)e->act_rows * sizeof(uint32_t)));
+    e->rows_cap = e->act_rows;
+  }
+  if (e->act_rows > 0) {
+    CUDA_TRY(cudaMemcpy(e->d_row_off, rows.row_off.data(), rows.row_off.size() * sizeof(int64_t),
+                        cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(e->d_row_n, rows.row_n.data(), rows.row_n.size() * sizeof(int32_t),
+                        cudaMemcpyHostToDevice));
+  }
   return NGAP_OK;
+}
+
+// One warp per activation row: the slots with a first match, in slot order.
+__global__ void act_compact(const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_n,
+                            int32_t nrows, const uint32_t* __restrict__ act,
+                            uint32_t* __restrict__ list, uint32_t* __restrict__ cnt) {
+  const int32_t row = (int32_t)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;  // whole warps
+  const int64_t off = row_off[row];
+  const int32_t n = row_n[row];
+  uint32_t c = 0;
+  for (int32_t i0 = 0; i0 < n; i0 += 32) {
+    const int32_t i = i0 + lane;
+    const bool ok = i < n && act[off + i] != 0xffffffffu;
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (ok) list[off + c + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+    c += __popc(m);
+  }
+  if (lane == 0) cnt[row] = c;
 }
 
 // The matching launches of a plan: the activation tiles' tasks, then the rest
@@ -537,6 +603,12 @@ int launch_plan(ngap_engine* e, MatchParams mp, int smem, cudaStream_t st) {
     CUDA_TRY(cudaGetLastError());
     e->launches++;
     CUDA_TRY(cudaMemsetAsync(mp.task_counter, 0, sizeof(unsigned int), st));
+  }
+  if (e->act_rows > 0) {
+    act_compact<<<(e->act_rows + 7) / 8, 256, 0, st>>>(e->d_row_off, e->d_row_n, e->act_rows,
+                                                       e->d_act, e->d_act_list, e->d_act_cnt);
+    CUDA_TRY(cudaGetLastError());
+    e->launches++;
   }
   if (e->ntasks > e->ntasks1) {
     mp.tasks = e->d_tasks + e->ntasks1;
@@ -854,10 +926,9 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     std::vector<UnitDev> units;
     std::vector<TaskDev> tasks;
     int32_t ntasks1 = 0;
-    int64_t act_entries = 0;
-    plan_units(t, key, full_grid, units, tasks, &ntasks1, &act_entries);
+    const ActRows rows = plan_units(t, key, full_grid, units, tasks, &ntasks1);
     e->ntasks1 = ntasks1;
-    e->act_entries = act_entries;
+    if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       cudaFree(e->d_units);
       e->d_units = nullptr;
@@ -888,7 +959,6 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   e->grid = grid;
   rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states, t->max_nact);
   if (rc != NGAP_OK) return rc;
-  if ((rc = ensure_act(e)) != NGAP_OK) return rc;
 
   CUDA_TRY(cudaEventRecord(e->ev[0], st));
   if (input_on_device)
@@ -925,6 +995,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.ovf_cap = e->ovf_cap;
   mp.work = e->d_counters + 2;
   mp.act = e->d_act;
+  mp.act_list = e->d_act_list;
+  mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
@@ -1196,7 +1268,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
         }
     }
     make_tasks(units, pass1, unbounded, bounded, full_grid, tasks, &e->ntasks1);
-    e->act_entries = rows.total;
+    if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       cudaFree(e->d_units);
       e->d_units = nullptr;
@@ -1231,7 +1303,6 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   e->grid = grid;
   if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states, ts->max_nact)) != NGAP_OK)
     return rc;
-  if ((rc = ensure_act(e)) != NGAP_OK) return rc;
 
   MatchParams mp;
   mp.tiles = ts->d_tiles;
@@ -1259,6 +1330,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   mp.ovf_cap = e->ovf_cap;
   mp.work = e->d_counters + 2;
   mp.act = e->d_act;
+  mp.act_list = e->d_act_list;
+  mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
 

@@ -78,6 +78,8 @@ struct MatchParams {
   unsigned long long* work; // [0] entries expanded, [1] entries injected
   uint32_t* act;            // activation slots (first match of sticky states, offset in the
                             // segment; 0xffffffff = none)
+  const uint32_t* act_list; // per row (segment of a pair): the slots that have a first match,
+  const uint32_t* act_cnt;  // at the row's offset, and their count
   uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
   int32_t stk_g_cap;        // kStickyCap
 };
@@ -125,6 +127,7 @@ struct WarpRun {
   uint32_t* marks;
   uint32_t* act;   // activation units: the segment's slots (reports become atomicMin)
   int stk_cap;     // capacity of the sticky list (ws.stk_s / stk_q)
+  bool stk_rep;    // layered units: some registered sticky state is a report state
 };
 
 // The tile a warp works on: hot tables in shared memory (or global memory
@@ -651,6 +654,85 @@ __device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem&
   __syncwarp();
 }
 
+// Layered tiles: the work of the unit's sticky states at window offsets
+// [r0, r0 + 32) (lanes over positions). The list holds activation slots
+// (stk_s) and first matches (stk_q); a slot's union mask (the classes any of
+// its successors accepts) rejects most positions before the successor
+// tables are read.
+__device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, WarpSmem& ws,
+                                                         WarpRun& w, const TileView& tv,
+                                                         const UnitCtx& c, int lane, int r0) {
+  const TileDev& t = *tv.t;
+  const int r = r0 + lane;
+  const bool valid = r < c.wlen;
+  const int64_t tp = c.wb + r;
+  const uint32_t sym = valid ? c.in[r] : 0u;
+  const bool need = valid && tp + 1 < c.hi;
+  const bool emit = valid && tp >= c.emit_lo;
+  if (w.stk_rep) {  // a reporting sticky state reports at every position after its first match
+    for (int i = 0; i < w.nstk; i++) {
+      const uint32_t s = __ldg(t.act_local + ws.stk_s[i]);
+      const bool rs = emit && tp > (int64_t)ws.stk_q[i] && is_report(tv, s);
+      emit_report(p, ws, w, lane, rs, rs ? __ldg(t.sid + s) : 0u, (uint32_t)tp);
+    }
+  }
+  const uint32_t word = sym >> 5, bit = 1u << (sym & 31);
+  int cnt = 0;
+  bool any_rep = false;
+  for (int i = 0; i < w.nstk; i++) {
+    if (!(valid && tp > (int64_t)ws.stk_q[i])) continue;
+    const uint32_t slot = ws.stk_s[i];
+    if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
+    const uint4 sc = load_succ(tv, __ldg(t.act_local + slot));
+    const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym)) {
+        cnt++;
+        any_rep |= (us[j] >> 31) && emit;
+      }
+  }
+  if (__any_sync(kFull, any_rep)) {
+    for (int i = 0; i < w.nstk; i++) {
+      const bool act = valid && tp > (int64_t)ws.stk_q[i];
+      const uint4 sc = load_succ(tv, __ldg(t.act_local + ws.stk_s[i]));
+      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+      bool ok[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        ok[j] = act && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
+      report4(p, ws, w, tv, lane, ok, us, tp, emit);
+    }
+  }
+  const int pc = need ? cnt : 0;
+  int incl = pc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  if (pc) {
+    int pos = w.top + incl - pc;
+    for (int i = 0; i < w.nstk; i++) {
+      if (tp <= (int64_t)ws.stk_q[i]) continue;
+      const uint32_t slot = ws.stk_s[i];
+      if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
+      const uint4 sc = load_succ(tv, __ldg(t.act_local + slot));
+      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t u = us[j] & kIdMask;
+        if (us[j] != kNoSucc && accepts(tv, u, sym))
+          store_entry(p, ws, w, pos++, (u << kEntryPosBits) | (uint32_t)r);
+      }
+    }
+  }
+  grow_stack(p, w, total);
+  __syncwarp();
+}
+
 // Expands the up-to-32 entries on top of the stack: one step of the worklist.
 template <int PRIV>
 __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, WarpRun& w,
@@ -801,6 +883,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   w.marks = p.marks + (size_t)slot * p.mark_words;
   w.act = nullptr;
   w.stk_cap = kStickyCap;
+  w.stk_rep = false;
   uint32_t* const stk_smem = ws.stk_s;
   if (lane == 0) {
     mbar_init(&ws.bar[0], 1);
@@ -903,29 +986,36 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       w.base = (uint32_t)un.base;
       w.act = t->phase == 1 ? p.act + un.act_row : nullptr;
       if (layered) {
-        // sticky states whose first match (from the activation pass) comes
-        // before the unit's end: active from there on; a reporting one also
-        // reports at its first match
-        for (int i0 = 0; i0 < t->nact; i0 += 32) {
-          const int i = i0 + lane;
-          const uint32_t f = i < t->nact ? p.act[un.act_row + i] : kNoAct;
+        // sticky states whose first match (from the activation pass; the
+        // segment's matched slots are listed at act_list) comes before the
+        // unit's end: active from there on; a reporting one also reports at
+        // its first match
+        const uint32_t n = p.act_cnt[un.act_rowid];
+        bool rep_any = false;
+        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+          const uint32_t i = i0 + lane;
+          const uint32_t slot = i < n ? p.act_list[un.act_row + i] : 0u;
+          const uint32_t f = i < n ? p.act[un.act_row + slot] : kNoAct;
           const int64_t q = un.base + (int64_t)f;
           const bool ok = f != kNoAct && q < c.hi;
           const unsigned m = __ballot_sync(kFull, ok);
-          const uint32_t sv = ok ? __ldg(t->act_local + i) : 0u;
+          const uint32_t sv = ok ? __ldg(t->act_local + slot) : 0u;
           if (ok) {
             const int k = w.nstk + __popc(m & lanemask_lt(lane));
             if (k < w.stk_cap) {
-              ws.stk_s[k] = sv;
+              ws.stk_s[k] = slot;
               ws.stk_q[k] = (uint32_t)q;
             } else {
               atomicOr(p.err, kErrQueue);
             }
           }
           w.nstk = min(w.nstk + __popc(m), w.stk_cap);
-          const bool rep = ok && is_report(tv, sv) && q >= c.emit_lo;
+          const bool rs = ok && is_report(tv, sv);
+          rep_any |= rs;
+          const bool rep = rs && q >= c.emit_lo;
           emit_report(p, ws, w, lane, rep, rep ? __ldg(t->sid + sv) : 0u, (uint32_t)q);
         }
+        w.stk_rep = __any_sync(kFull, rep_any);
         __syncwarp();
       }
       int cur = 0;
@@ -976,7 +1066,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
                         (uint32_t)un.lo);
             const bool need = ok && un.lo + 1 < c.hi;
             bool reg = false;
-            if (tv.sticky)
+            if (layered)  // already registered from the activation pass
+              reg = is_sticky(tv, v);
+            else if (tv.sticky)
               reg = register_each(p, ws, w, tv, c, lane, need && is_sticky(tv, v), v, un.lo, wb);
             push_entry(p, ws, w, lane, need && !reg, v << kEntryPosBits);
           }
@@ -996,7 +1088,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
               continue;
             }
             if (scur < c.wlen) {
-              sticky_positions(p, ws, w, tv, c, lane, scur, 32);
+              layered_sticky_positions(p, ws, w, tv, c, lane, scur);
               scur += 32;
               continue;
             }

@@ -559,6 +559,18 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
     }
   }
   for (uint32_t w : t.sticky) t.nsticky += __builtin_popcount(w);
+  if (variant == kLayered) {  // union of the successors' class masks of every slot
+    t.stk_union.assign((size_t)t.nact * t.cw, 0);
+    for (int32_t i = 0; i < t.nact; i++) {
+      const uint32_t s = t.act_local[i];
+      for (int j = 0; j < 4; j++) {
+        const uint32_t u = t.succ[(size_t)s * 4 + j];
+        if (u == kNoSucc) continue;
+        for (int k = 0; k < t.cw; k++)
+          t.stk_union[(size_t)i * t.cw + k] |= t.cmask[(size_t)(u & 0x7fffffffu) * t.cw + k];
+      }
+    }
+  }
   build_prefix_tables(t, opts, global);
   build_image(t);
   tiles.push_back(std::move(t));

@@ -33,6 +33,7 @@ struct TileHost {
   int32_t pair = -1;                 // activation/layered tiles: index of their pair
   int32_t nact = 0;                  // activation slots (sticky states) of the pair
   std::vector<uint32_t> act_local;   // layered: local id of the sticky state of each slot
+  std::vector<uint32_t> stk_union;   // layered: [nact][cw] classes any successor of the slot accepts
   std::vector<uint8_t> cls;          // 256: byte -> class, live classes first
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
   std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
