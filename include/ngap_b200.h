@@ -171,6 +171,40 @@ int ngap_last_times_ms(const ngap_engine* e, float* match_ms, float* sort_ms);
 int ngap_last_launches(const ngap_engine* e);
 /* Worklist entries expanded and always-active entries injected by the last match. */
 int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injected);
+/* Bytes of device memory the engine holds (input copy, reports, per-warp scratch). */
+int64_t ngap_engine_device_bytes(const ngap_engine* e);
+
+/* ---- worklist traces ---- */
+
+/* Generalises --motivate-worklist-length (code/src/ngap/kernel_ngap_OA.cu:366-369,
+ * code/src/ngap/ngap.cu:1843-1866), which records the fetched worklist length
+ * per round: with tracing on, every later match (plain or batched) records
+ * the worklist work of each unit (one tile over one chunk of a segment or
+ * stream). */
+typedef struct ngap_unit_trace {
+  int32_t stream;   /* segment (ngap_match) or stream (ngap_batch_match) index */
+  int32_t tile;     /* tile index (in the tableset for batched matches) */
+  int64_t lo, hi;   /* positions whose reports the unit owns, relative to its segment/stream */
+  uint64_t work;    /* worklist entries the unit expanded plus entries it injected */
+} ngap_unit_trace;
+int ngap_engine_set_trace(ngap_engine* e, int enable);
+/* Copies the last match's unit records (after ngap_engine_sync); *n = count. */
+int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* n);
+
+/* Statistics of built tables, the NFA features of the cost model. The
+ * reference sizes its adaptive AAS interval from the longest table list
+ * (maxkey, code/src/ngap/kernel_ngap_OA.cu:180-194). */
+typedef struct ngap_tables_stats {
+  int32_t tiles, states, edges, aas;
+  int32_t depth;          /* deepest prefix table */
+  int32_t max_nlive;      /* live byte classes (key base) */
+  int32_t max_list;       /* longest list of a deepest table (maxkey) */
+  int32_t cutoff;         /* sum over tiles of the mean non-empty deepest list length */
+  int64_t list_entries;   /* entries of the deepest tables, all tiles */
+  double exp_list;        /* sum over tiles of the deepest tables' mean list length per key
+                             (all keys equally likely): states injected per position */
+} ngap_tables_stats;
+int ngap_tables_stats_get(const ngap_tables* t, ngap_tables_stats* out);
 
 /* ---- batched matching: many streams, several NFAs, one launch ---- */
 
@@ -187,7 +221,7 @@ typedef struct ngap_batch_stream {
   uint64_t offset;  /* first byte of the stream in the batch input */
   uint64_t length;  /* bytes; the stream is one segment (start-of-data states at its start) */
   int32_t nfa;      /* index into the tableset */
-  int32_t pad;
+  int32_t chunk;    /* chunk length for this stream's acyclic tiles; 0 = the batch's */
 } ngap_batch_stream;
 
 typedef struct ngap_batch_params {
@@ -200,6 +234,8 @@ typedef struct ngap_batch_params {
   int chunk;                /* 0 = automatic */
   int use_graph;            /* capture the pipeline in a CUDA graph; replay it while the
                                tableset, streams, parameters and input pointer repeat */
+  int queue_capacity;       /* overflow-stack entries per warp (>= 1024); 0 = 65536. A run
+                               that needs more fails with NGAP_E_OVERFLOW_QUEUE */
 } ngap_batch_params;
 
 /* Matches every stream against its NFA in one persistent launch, then sorts
@@ -212,6 +248,43 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
  * not NULL, the stream index of each; *n receives the count copied. */
 int ngap_batch_results(ngap_engine* e, uint64_t* reports, uint32_t* stream_ids, uint64_t cap,
                        uint64_t* n);
+
+/* ---- learned cost model ---- */
+
+/* The reference has no cost model: it records the fetched worklist length per
+ * round (--motivate-worklist-length, code/src/ngap/kernel_ngap_OA.cu:366-369)
+ * and sizes its adaptive AAS interval from the longest table list
+ * (kernel_ngap_OA.cu:180-194). These entry points compute input features and
+ * train / run a small regressor on the engine's own worklist traces
+ * (ngap_trace_copy); the scheduler above them (ngap_b200/cost_model.py)
+ * predicts worklist entries per input byte. */
+#define NGAP_FEAT_BYTES 258 /* 256-bin histogram, mean and max windowed entropy */
+
+/* Features of n regions of data (device or host memory of `bytes` bytes):
+ * region i (offsets[i], lengths[i]) gets out[i * NGAP_FEAT_BYTES + k]: the
+ * symbol histogram normalised to sum 1 (k < 256), then the mean (k = 256) and
+ * the largest (k = 257) Shannon entropy of its windows of `window` bytes, in
+ * bits / 8. out is host memory; the call waits for the result. */
+int ngap_features(const uint8_t* data, uint64_t bytes, int on_device, const uint64_t* offsets,
+                  const uint64_t* lengths, int n, int window, float* out, void* stream);
+
+/* A regressor with two hidden ReLU layers of `hidden` (= 64) units and one
+ * linear output; FP32 parameters on the device. */
+typedef struct ngap_mlp ngap_mlp;
+int ngap_mlp_create(int device, int in_dim, int hidden, uint64_t seed, ngap_mlp** out);
+void ngap_mlp_destroy(ngap_mlp* m);
+/* Adam on the mean squared error over x[n][in_dim], y[n] (host arrays):
+ * `epochs` shuffled passes in mini-batches of `batch`; *loss receives the
+ * last epoch's mean squared error. FP32 throughout. */
+int ngap_mlp_train(ngap_mlp* m, const float* x, const float* y, int64_t n, int epochs, int batch,
+                   float lr, float* loss);
+/* y[n] = model(x[n][in_dim]) (host arrays). bf16 = 1 rounds inputs, weights and
+ * activations to bfloat16 (FP32 accumulation); 0 computes in FP32. Runs on
+ * the model's own stream; allocates only when n exceeds every earlier call. */
+int ngap_mlp_predict(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y);
+/* Parameters as one FP32 vector; *n = count (out = NULL queries it). */
+int ngap_mlp_get_params(const ngap_mlp* m, float* out, int64_t cap, int64_t* n);
+int ngap_mlp_set_params(ngap_mlp* m, const float* in, int64_t n);
 
 /* ---- report compaction ---- */
 

@@ -64,14 +64,30 @@ class MatchParams(ctypes.Structure):
 
 class BatchStream(ctypes.Structure):
     _fields_ = [("offset", ctypes.c_uint64), ("length", ctypes.c_uint64),
-                ("nfa", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("nfa", ctypes.c_int32), ("chunk", ctypes.c_int32)]
 
 
 class BatchParams(ctypes.Structure):
     _fields_ = [("algorithm", ctypes.c_int), ("unique", ctypes.c_int),
                 ("active_threshold", ctypes.c_int), ("report_off", ctypes.c_int),
                 ("result_capacity", ctypes.c_uint64), ("window", ctypes.c_int),
-                ("chunk", ctypes.c_int), ("use_graph", ctypes.c_int)]
+                ("chunk", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("queue_capacity", ctypes.c_int)]
+
+
+class UnitTrace(ctypes.Structure):
+    _fields_ = [("stream", ctypes.c_int32), ("tile", ctypes.c_int32), ("lo", ctypes.c_int64),
+                ("hi", ctypes.c_int64), ("work", ctypes.c_uint64)]
+
+
+class TablesStats(ctypes.Structure):
+    _fields_ = [("tiles", ctypes.c_int32), ("states", ctypes.c_int32), ("edges", ctypes.c_int32),
+                ("aas", ctypes.c_int32), ("depth", ctypes.c_int32), ("max_nlive", ctypes.c_int32),
+                ("max_list", ctypes.c_int32), ("cutoff", ctypes.c_int32),
+                ("list_entries", ctypes.c_int64), ("exp_list", ctypes.c_double)]
+
+
+FEAT_BYTES = 258  # NGAP_FEAT_BYTES
 
 
 # name -> (restype, argtypes); exactly the functions include/ngap_b200.h declares
@@ -109,6 +125,25 @@ SIGNATURES = {
     "ngap_last_launches": (ctypes.c_int, [ctypes.c_void_p]),
     "ngap_engine_work": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "ngap_engine_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
+    "ngap_engine_set_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ngap_trace_copy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(UnitTrace), ctypes.c_int64,
+                                       ctypes.POINTER(ctypes.c_int64)]),
+    "ngap_tables_stats_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TablesStats)]),
+    "ngap_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_void_p]),
+    "ngap_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "ngap_mlp_destroy": (None, [ctypes.c_void_p]),
+    "ngap_mlp_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                      ctypes.POINTER(ctypes.c_float)]),
+    "ngap_mlp_predict": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_int, ctypes.c_void_p]),
+    "ngap_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                           ctypes.POINTER(ctypes.c_int64)]),
+    "ngap_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
     "ngap_tableset_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_void_p)]),
     "ngap_tableset_destroy": (None, [ctypes.c_void_p]),

@@ -96,7 +96,7 @@ struct UnitDev {
   uint64_t key_hi;   // stream index, already shifted into the report key
   int64_t act_row;   // phase 1 and 2 tiles: first activation slot of the unit's segment
   int32_t act_rowid; // its row (pair, segment) in the compacted activation lists
-  int32_t pad;
+  int32_t stream;    // segment (plain matching) or stream (batched matching) index
 };
 
 // A CTA-level task: consecutive units [ubegin, uend) of one tile.

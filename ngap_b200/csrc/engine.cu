@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <tuple>
 #include <vector>
@@ -34,6 +35,7 @@ namespace {
 // work, [5..6] the standalone sort's counts, [kRadixCount] keys left to the
 // radix pipeline after the small-set sort.
 constexpr int kNumCounters = 16;
+constexpr int kDefaultQueue = 1 << 16;  // overflow-stack entries per warp
 constexpr int kRadixCount = 8;
 
 int bits_for(uint64_t x) {  // bits needed to hold values < x (x >= 1)
@@ -121,6 +123,12 @@ struct ngap_engine {
   size_t tasks_cap = 0;
   int32_t ntasks = 0;
   int32_t ntasks1 = 0;       // tasks of activation tiles, launched first
+  // worklist traces
+  bool trace = false;
+  unsigned long long* d_unit_work = nullptr;
+  size_t unit_work_cap = 0;
+  std::vector<UnitDev> h_units;  // the current plan's units (host copy)
+  int64_t trace_seg_len = 0;     // plain matching: unit positions are made segment-relative
   int64_t act_entries = 0;   // activation slots the plan uses
   uint32_t* d_act = nullptr;
   uint32_t* d_act_list = nullptr;  // per row: slots with a first match (compacted)
@@ -191,6 +199,7 @@ struct ngap_engine {
     cudaFree(d_carry);
     cudaFree(d_marks);
     cudaFree(d_ovf);
+    cudaFree(d_unit_work);
     cudaFree(d_act);
     cudaFree(d_act_list);
     cudaFree(d_row_off);
@@ -369,10 +378,14 @@ int ensure_reports(ngap_engine* e, uint64_t cap) {
   return NGAP_OK;
 }
 
-int ensure_slots(ngap_engine* e, size_t slots, int max_states, int max_nact) {
+int ensure_slots(ngap_engine* e, size_t slots, int max_states, int max_nact, int ovf_cap) {
   int carry_cap = std::max(max_states, 32);
   int mark_words = (max_states + 31) / 32 + 1;
-  int ovf_cap = 1 << 16;
+  if (ovf_cap != e->ovf_cap && e->d_ovf) {  // queue capacity changed: reallocate everything
+    e->slots = std::max(e->slots, slots);
+    slots = e->slots;
+    e->carry_cap = 0;
+  }
   const int stk_cap = max_nact > kStickyCap ? max_nact : 0;
   if (slots <= e->slots && stk_cap > e->stk_cap) {  // only the sticky lists grow
     cudaFree(e->d_stk);
@@ -417,6 +430,7 @@ struct SegSpec {
   bool starts;      // start-of-data states active at lo
   uint64_t key_hi;  // stream index in the report key
   int64_t base;     // offsets in reports are relative to this
+  int32_t index;    // segment or stream index
 };
 
 void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int chunk_opt,
@@ -428,6 +442,7 @@ void add_units(const TileHost& th, int tile, const SegSpec& s, int window, int c
   u.base = s.base;
   u.act_row = act.first;
   u.act_rowid = act.second;
+  u.stream = s.index;
   std::vector<UnitDev>& chunks = th.phase == 1 ? pass1 : bounded;
   const bool starts = s.starts && !th.start.empty();
   if (th.max_path < 0) {
@@ -500,11 +515,22 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
     return std::max<int64_t>(kWarpsPerCta,
                              std::min<int64_t>(512, (int64_t)n / std::max(1, 4 * grid)));
   };
+  // a task holds at most `per` units and, past its first unit, about a
+  // 16 * grid-th of the range's positions (at least 64 KiB), so that long
+  // chunks do not make long tasks
   auto cut = [&](size_t b, size_t e, int64_t per) {
+    int64_t total = 0;
+    for (size_t k = b; k < e; k++) total += units[k].hi - units[k].lo;
+    const int64_t cap = std::max<int64_t>(1 << 16, total / std::max(1, 16 * grid));
     size_t i = b;
     while (i < e) {
       size_t j = i;
-      while (j < e && units[j].tile == units[i].tile && (int64_t)(j - i) < per) j++;
+      int64_t bytes = 0;
+      while (j < e && units[j].tile == units[i].tile && (int64_t)(j - i) < per &&
+             (j == i || bytes + (units[j].hi - units[j].lo) <= cap)) {
+        bytes += units[j].hi - units[j].lo;
+        j++;
+      }
       TaskDev tk;
       tk.tile = units[i].tile;
       tk.ubegin = (int32_t)i;
@@ -527,13 +553,29 @@ ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
     for (int64_t s = 0; s < k.num_seg; s++) {
       SegSpec sp{s * k.seg_len, (s + 1) * k.seg_len, k.first_seg + s == 0 || k.is_dup != 0, 0ull,
-                 0};
+                 0, (int32_t)s};
       add_units(t->tiles[ti], ti, sp, k.window, k.chunk, rows.row(0, t->tiles[ti], s), pass1,
                 unbounded, bounded);
     }
   }
   make_tasks(units, pass1, unbounded, bounded, grid, tasks, ntasks1);
   return rows;
+}
+
+// Per-unit work counters when tracing (zeroed on st); null otherwise.
+int trace_buffer(ngap_engine* e, cudaStream_t st, unsigned long long** out) {
+  *out = nullptr;
+  if (!e->trace || e->nunits == 0) return NGAP_OK;
+  if ((size_t)e->nunits > e->unit_work_cap) {
+    cudaFree(e->d_unit_work);
+    e->d_unit_work = nullptr;
+    e->unit_work_cap = 0;
+    CUDA_TRY(cudaMalloc(&e->d_unit_work, (size_t)e->nunits * sizeof(unsigned long long)));
+    e->unit_work_cap = (size_t)e->nunits;
+  }
+  CUDA_TRY(cudaMemsetAsync(e->d_unit_work, 0, (size_t)e->nunits * sizeof(unsigned long long), st));
+  *out = e->d_unit_work;
+  return NGAP_OK;
 }
 
 // Activation buffers of a plan (slots, compacted lists, row table).
@@ -628,8 +670,19 @@ __global__ void swap_halves(uint64_t* a, uint64_t n) {
   }
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel function
+// (per device, shared by every engine of the process), so it only ever grows.
+std::mutex g_smem_mu;
+int g_smem_set[64];
+
 int set_smem(ngap_engine* e, int smem) {
   if (e->max_smem_set >= smem) return NGAP_OK;
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  const int dev = e->device & 63;
+  if (g_smem_set[dev] >= smem) {
+    e->max_smem_set = g_smem_set[dev];
+    return NGAP_OK;
+  }
   cudaError_t ce = cudaFuncSetAttribute(match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (ce == cudaSuccess)
     ce = cudaFuncSetAttribute(match_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -639,6 +692,7 @@ int set_smem(ngap_engine* e, int smem) {
     set_error("shared memory request of %d bytes rejected: %s", smem, cudaGetErrorString(ce));
     return NGAP_E_CUDA;
   }
+  g_smem_set[dev] = smem;
   e->max_smem_set = smem;
   return NGAP_OK;
 }
@@ -950,6 +1004,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
       CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
                           cudaMemcpyHostToDevice));
     e->nunits = (int32_t)units.size();
+    e->h_units = units;
     e->ntasks = (int32_t)tasks.size();
     e->plan_tables = t->serial;
     e->plan_key = key;
@@ -957,7 +1012,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   }
   const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
-  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states, t->max_nact);
+  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states, t->max_nact, kDefaultQueue);
   if (rc != NGAP_OK) return rc;
 
   CUDA_TRY(cudaEventRecord(e->ev[0], st));
@@ -999,6 +1054,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
+  if ((rc = trace_buffer(e, st, &mp.unit_work)) != NGAP_OK) return rc;
+  e->trace_seg_len = p->seg_len;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
   if (e->ntasks > 0) {
     if (priv == 0) rc = launch_plan<0>(e, mp, smem, st);
@@ -1088,6 +1145,84 @@ int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injecte
   if (!e) return NGAP_E_INVALID;
   if (expanded) *expanded = e->h_counters[2];
   if (injected) *injected = e->h_counters[3];
+  return NGAP_OK;
+}
+
+int64_t ngap_engine_device_bytes(const ngap_engine* e) {
+  if (!e) return 0;
+  int64_t b = (int64_t)e->input_cap + 3 * 8 * (int64_t)e->rep_cap + 4 * (int64_t)e->hist_cap;
+  b += (int64_t)e->slots * 4 * ((int64_t)e->carry_cap + e->mark_words + e->ovf_cap + 2 * e->stk_cap);
+  b += 8 * (int64_t)e->act_cap + 16 * (int64_t)e->rows_cap + 8 * (int64_t)e->unit_work_cap;
+  b += (int64_t)sizeof(UnitDev) * (int64_t)e->units_cap + (int64_t)sizeof(TaskDev) * (int64_t)e->tasks_cap;
+  b += 4 * (int64_t)e->stream_ids_cap;
+  return b;
+}
+
+int ngap_engine_set_trace(ngap_engine* e, int enable) {
+  if (!e) {
+    set_error("ngap_engine_set_trace: null engine");
+    return NGAP_E_INVALID;
+  }
+  e->trace = enable != 0;
+  return NGAP_OK;
+}
+
+int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* n) {
+  if (!e || !n || (!out && cap > 0)) {
+    set_error("ngap_trace_copy: bad argument");
+    return NGAP_E_INVALID;
+  }
+  *n = 0;
+  if (!e->trace || !e->ran || e->nunits == 0 || !e->d_unit_work) return NGAP_OK;
+  std::vector<unsigned long long> work(e->nunits);
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaMemcpy(work.data(), e->d_unit_work, work.size() * sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost));
+  const int64_t m = std::min<int64_t>(cap, e->nunits);
+  for (int64_t i = 0; i < m; i++) {
+    const UnitDev& u = e->h_units[i];
+    const int64_t base = e->trace_seg_len > 0 ? (int64_t)u.stream * e->trace_seg_len : u.base;
+    out[i].stream = u.stream;
+    out[i].tile = u.tile;
+    out[i].lo = u.emit_lo - base;
+    out[i].hi = u.hi - base;
+    out[i].work = work[i];
+  }
+  *n = m;
+  return NGAP_OK;
+}
+
+int ngap_tables_stats_get(const ngap_tables* t, ngap_tables_stats* out) {
+  if (!t || !out) {
+    set_error("ngap_tables_stats_get: null argument");
+    return NGAP_E_INVALID;
+  }
+  ngap_tables_stats st{};
+  st.tiles = (int32_t)t->tiles.size();
+  for (const TileHost& th : t->tiles) {
+    if (th.phase == 1) continue;  // activation tiles repeat states of their layered pair
+    st.states += th.nstates;
+    for (uint32_t u : th.succ) st.edges += u != kNoSucc ? 1 : 0;
+    st.aas += (int32_t)th.aas.size();
+    st.depth = std::max(st.depth, th.depth);
+    st.max_nlive = std::max(st.max_nlive, th.nlive);
+    const PrefixTableHost& pt = th.pt[th.depth - 1];
+    st.list_entries += (int64_t)pt.vlist.size();
+    st.cutoff += pt.cutoff;
+    double space = 1.0;
+    for (int d = 0; d < th.depth; d++) space *= (double)std::max(1, th.nlive);
+    st.exp_list += (double)pt.vlist.size() / space;
+    if (pt.dense) {
+      for (size_t k = 0; k + 1 < pt.voff.size(); k++)
+        st.max_list = std::max<int32_t>(st.max_list, (int32_t)(pt.voff[k + 1] - pt.voff[k]));
+    } else {
+      for (size_t k = 0; k < pt.slots.size() / 4; k++)
+        if (pt.slots[k * 4] != kHashEmpty)
+          st.max_list = std::max<int32_t>(st.max_list, (int32_t)(pt.slots[k * 4 + 3] >> 16));
+    }
+  }
+  *out = st;
   return NGAP_OK;
 }
 
@@ -1243,7 +1378,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     if (e->batch_streams.size() != sv.size()) return false;
     for (size_t i = 0; i < sv.size(); i++)
       if (sv[i].offset != e->batch_streams[i].offset || sv[i].length != e->batch_streams[i].length ||
-          sv[i].nfa != e->batch_streams[i].nfa)
+          sv[i].nfa != e->batch_streams[i].nfa || sv[i].chunk != e->batch_streams[i].chunk)
         return false;
     return true;
   };
@@ -1262,9 +1397,10 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
           const ngap_batch_stream& s = sv[si];
           if (s.length == 0) continue;
           SegSpec sp{(int64_t)s.offset, (int64_t)(s.offset + s.length), true,
-                     (uint64_t)si << sshift, (int64_t)s.offset};
-          add_units(t->tiles[ti], ts->tile_base[n] + ti, sp, window, p->chunk,
-                    rows.row((int)n, t->tiles[ti], si), pass1, unbounded, bounded);
+                     (uint64_t)si << sshift, (int64_t)s.offset, si};
+          add_units(t->tiles[ti], ts->tile_base[n] + ti, sp, window,
+                    s.chunk > 0 ? s.chunk : p->chunk, rows.row((int)n, t->tiles[ti], si), pass1,
+                    unbounded, bounded);
         }
     }
     make_tasks(units, pass1, unbounded, bounded, full_grid, tasks, &e->ntasks1);
@@ -1290,6 +1426,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
       CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
                           cudaMemcpyHostToDevice));
     e->nunits = (int32_t)units.size();
+    e->h_units = units;
     e->ntasks = (int32_t)tasks.size();
     e->plan_tables = 0;  // the plain plan cache no longer describes the buffers
     e->plan_key = UnitPlanKey{-1, -1, -1, -1, -1, -1};
@@ -1301,7 +1438,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   }
   const int grid = std::max(1, std::min(full_grid, e->ntasks));
   e->grid = grid;
-  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states, ts->max_nact)) != NGAP_OK)
+  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states, ts->max_nact,
+                         p->queue_capacity > 0 ? std::max(p->queue_capacity, 1024) : kDefaultQueue)) != NGAP_OK)
     return rc;
 
   MatchParams mp;
@@ -1334,8 +1472,14 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
+  mp.unit_work = nullptr;
+  e->trace_seg_len = 0;
 
   auto enqueue = [&](cudaStream_t qs) -> int {
+    if (e->trace) {
+      const int r = trace_buffer(e, qs, &mp.unit_work);
+      if (r != NGAP_OK) return r;
+    }
     if (input_on_device)
       CUDA_TRY(cudaMemcpyAsync(e->d_input, input, input_bytes, cudaMemcpyDeviceToDevice, qs));
     else
@@ -1387,7 +1531,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   std::vector<uint64_t> key = {ts->serial, (uint64_t)(uintptr_t)input, input_bytes,
                                (uint64_t)input_on_device, (uint64_t)p->algorithm,
                                (uint64_t)p->unique, (uint64_t)p->active_threshold,
-                               (uint64_t)p->report_off, cap, (uint64_t)window, (uint64_t)p->chunk};
+                               (uint64_t)p->report_off, cap, (uint64_t)window, (uint64_t)p->chunk,
+                               (uint64_t)e->trace, (uint64_t)e->ovf_cap};
   if (replanned || !e->graph || key != e->graph_key) {
     if (e->graph) {
       cudaGraphExecDestroy(e->graph);

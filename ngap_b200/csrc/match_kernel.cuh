@@ -82,6 +82,7 @@ struct MatchParams {
   const uint32_t* act_cnt;  // at the row's offset, and their count
   uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
   int32_t stk_g_cap;        // kStickyCap
+  unsigned long long* unit_work;  // [units]: entries expanded + injected per unit (tracing), or null
 };
 
 constexpr uint32_t kNoAct = 0xffffffffu;
@@ -978,6 +979,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       uid = __shfl_sync(kFull, uid, 0);
       if (uid >= (unsigned)tk.uend) break;
       const UnitDev un = p.units[uid];
+      const unsigned long long work0 = n_expanded + n_injected;  // per-unit trace
       UnitCtx c;
       c.hi = un.hi;
       c.emit_lo = un.emit_lo;
@@ -1109,6 +1111,12 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         }
         inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
         cur ^= 1;
+      }
+      if (p.unit_work) {  // worklist work of this unit (all lanes)
+        unsigned long long d = n_expanded + n_injected - work0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+        if (lane == 0) p.unit_work[uid] = d;
       }
       if (dead) {
         for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;

@@ -134,6 +134,13 @@ class Tables:
     def device_bytes(self):
         return lib().ngap_tables_device_bytes(self._h)
 
+    def stats(self):
+        """Table statistics (dict): tiles, states, edges, aas, depth, max_nlive,
+        max_list, cutoff, list_entries, exp_list."""
+        st = _lib.TablesStats()
+        check(lib().ngap_tables_stats_get(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.TablesStats._fields_}
+
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
             _lib._lib.ngap_tables_destroy(self._h)
@@ -172,6 +179,26 @@ class Engine:
 
     def sync(self):
         return check(lib().ngap_engine_sync(self._h))
+
+    def set_trace(self, enable=True):
+        """Records per-unit worklist work in the following matches."""
+        check(lib().ngap_engine_set_trace(self._h, int(bool(enable))))
+
+    def unit_trace(self):
+        """Records of the last match's units: numpy structured array with
+        fields stream, tile, lo, hi (positions relative to the segment or
+        stream) and work (entries expanded + injected)."""
+        n = ctypes.c_int64()
+        cap = 1 << 22
+        buf = (_lib.UnitTrace * cap)()
+        check(lib().ngap_trace_copy(self._h, buf, cap, ctypes.byref(n)))
+        dt = np.dtype([("stream", np.int32), ("tile", np.int32), ("lo", np.int64),
+                       ("hi", np.int64), ("work", np.uint64)])
+        return np.frombuffer(buf, dtype=dt, count=n.value).copy()
+
+    @property
+    def device_bytes(self):
+        return lib().ngap_engine_device_bytes(self._h)
 
     def match(self, tables, data, num_seg, seg_len, **kw):
         self.match_async(tables, data, num_seg, seg_len, **kw)
@@ -245,18 +272,21 @@ class TableSet:
 def batch_match_async(engine, tableset, data, offsets, lengths, nfas,
                       algorithm="nonblockingpcgroups", unique=False, active_threshold=20,
                       report_off=False, result_capacity=54619400, window=0, chunk=0,
-                      use_graph=False, stream=None):
+                      use_graph=False, stream=None, chunks=None, queue_capacity=0):
     """Starts one launch over all streams: stream i is data[offsets[i] :
     offsets[i] + lengths[i]] matched against tableset NFA nfas[i]. `data` is a
-    numpy uint8 array (pinned memory is needed with use_graph) or a CUDA tensor."""
+    numpy uint8 array (pinned memory is needed with use_graph) or a CUDA tensor.
+    chunks: optional per-stream chunk lengths (0 = `chunk`); queue_capacity:
+    overflow-stack entries per warp (0 = the default)."""
     n = len(offsets)
     ss = (_lib.BatchStream * n)()
     for i in range(n):
-        ss[i] = _lib.BatchStream(int(offsets[i]), int(lengths[i]), int(nfas[i]), 0)
+        ss[i] = _lib.BatchStream(int(offsets[i]), int(lengths[i]), int(nfas[i]),
+                                 int(chunks[i]) if chunks is not None else 0)
     engine._keep_streams = ss
     algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
     p = _lib.BatchParams(algo, int(unique), active_threshold, int(report_off), result_capacity,
-                         window, chunk, int(use_graph))
+                         window, chunk, int(use_graph), int(queue_capacity))
     if hasattr(data, "data_ptr"):
         ptr, on_dev, nbytes = data.data_ptr(), int(getattr(data, "is_cuda", True)), data.numel()
     else:
