@@ -371,6 +371,106 @@ def run_batched(args, warmup, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+SERVE_DESC = ("Poisson requests at 2000/s, NFA uniform over the 16 of the batched suite, "
+              "length log-normal (median 64 KiB, sigma 1.5), 2 engine slots, 1 GiB in-flight "
+              "budget")
+SERVE_STEP_S = 0.25  # seconds of arrivals per step
+
+
+def run_serving(args, warmup, rank):
+    """Serving: p50/p99 latency and served MB/s under the default, static and
+    learned schedulers, and the frontier-prediction error of each predictor."""
+    import torch
+    import ngap_b200 as nb
+    from ngap_b200 import cost_model as cm, serving as sv, workloads as W
+
+    if rank != 0:  # one GPU: replicas of a latency measurement say nothing more
+        return
+    torch.cuda.set_device(0)
+    nfas, data, offsets, lengths, nfa_of = W.batched_suite(seed=4)
+    groups = [nb.Groups(nb.Nfa.from_string(n["anml"]), group_num=1) for n in nfas]
+    tables = [nb.Tables(g, precompute_depth=-1) for g in groups]
+    ts = nb.TableSet(tables)
+    eng = nb.Engine(0)
+    d = torch.from_numpy(data).cuda()
+    reg = cm.region_table(d, offsets, lengths, nfa_of, tables)
+    y = cm.collect(eng, ts, d, offsets, lengths, nfa_of, reg)
+    del d
+    test = np.random.default_rng(0).random(len(offsets)) < 0.3
+    te = test[reg["stream"]]
+    lm = cm.LearnedModel(0).fit(reg["x"][~te], y[~te], epochs=60)
+    mean = cm.NfaMeanModel(len(nfas)).fit(reg["nfa"][~te], y[~te], reg["len"][~te])
+    stat = cm.StaticModel(reg["stats"])
+    err = {}
+    for name, pr in (("static", stat.predict(reg["nfa"])), ("nfa_mean", mean.predict(reg["nfa"])),
+                     ("learned_fp32", lm.predict(reg["nfa"], reg["x"], bf16=False)),
+                     ("learned_bf16", lm.predict(reg["nfa"], reg["x"], bf16=True))):
+        e = cm.relative_error(pr[te], y[te])
+        err[name] = {"median": float(np.median(e)), "mean": float(np.mean(e))}
+    pool = [data[int(o):int(o + l)] for o, l in zip(offsets, lengths)]
+    dur = SERVE_STEP_S * args.steps
+    reqs = sv.make_requests(pool, nfa_of, len(nfas), rate=2000, duration=dur, seed=5)
+    warm = sv.make_requests(pool, nfa_of, len(nfas), rate=2000, duration=SERVE_STEP_S * warmup,
+                            seed=6)
+    preds = {"default": None, "static": sv.Predictor("static", tables),
+             "learned": sv.Predictor("learned", tables, lm)}
+    servers = {}
+    for name, pred in preds.items():
+        q = cm.queue_for(float(np.max(pred.density(warm)))) if pred else 0
+        srv = sv.Server(ts, predictor=pred, slots=2, budget=1 << 30, queue_capacity=q)
+        srv.run([sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in warm])
+        servers[name] = (srv, q)
+    # two interleaved rounds of the three schedulers (single runs are noisy)
+    lat = {name: [] for name in preds}
+    served, launches, clk_all, dev_ms = {}, 0, None, 0.0
+    for rnd in range(2):
+        for name, (srv, q) in servers.items():
+            srv.batches.clear()
+            srv.launches = 0
+            rs = [sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in reqs]
+            with ClockSampler(0) as clk:
+                m = srv.run(rs)
+            launches += srv.launches
+            lat[name].append({"p50_ms": m["p50_ms"], "p99_ms": m["p99_ms"],
+                              "mean_ms": m["mean_ms"], "batches": m["batches"],
+                              "queue_capacity": q})
+            served[name] = m["MBps"]
+            if name == "learned" and rnd == 1:
+                clk_all = clk.summary()
+                dev_ms = sum(b[3] for b in srv.batches)
+    total = sum(len(r.data) for r in reqs)
+    peak, peak_kind = load_peaks()
+    line = {"metric": METRIC + "; serving p50/p99 latency", "value": served["learned"],
+            "unit": "MB/s", "n_gpus": 1, "steps": args.steps, "warmup": warmup,
+            "ms_per_step": SERVE_STEP_S * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generators, same shapes as the benchmark config)",
+            "config": {"workload": "serving", "desc": SERVE_DESC, "requests": len(reqs),
+                       "seconds_of_arrivals": dur, "bytes": total, "rounds": 2,
+                       "timing": "wall clock from arrival to reports on the host"},
+            "latency_ms": lat, "served_mbps": served,
+            "scheduler": "requests in arrival order; static/learned shorten the chunks of "
+                         "requests predicted denser than 2 entries per byte (never longer than "
+                         "the default 2048) and size the queue from the densest prediction",
+            "frontier_prediction_rel_err": err,
+            "gpu_launches": launches, "clocks": clk_all,
+            "e2e": {"value": served["learned"], "unit": "MB/s", "h2d_bytes_per_step":
+                    int(total / max(1, args.steps)), "d2h_bytes_per_step": None},
+            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                         "kernel": "match_kernel (batched, learned scheduler)",
+                         "achieved": total / (dev_ms / 1e3) / 1e9 if dev_ms else None,
+                         "frac": total / (dev_ms / 1e3) / 1e9 / peak if dev_ms else None,
+                         "note": "input bytes over the device time of the served batches; the "
+                                 "device is mostly idle at this offered load",
+                         "traffic": None}}
+    if not args.no_cpu_baseline:
+        cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of)
+        cb.pop("stats")
+        cb.pop("bytes")
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+
+
 def run_batched_reference(args, warmup):
     """Reference arm of the batched suite: the reference CPU matcher (the
     oracle's restatement) over bounded samples of the streams, all host threads."""
@@ -413,6 +513,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "serving":
+        if args.impl == "reference":
+            if rank == 0:
+                run_batched_reference(args, warmup)
+            return
+        run_serving(args, warmup, rank)
+        return
 
     if args.workload == "batched_suite":
         if args.impl == "reference":

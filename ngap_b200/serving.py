@@ -16,10 +16,11 @@ single 1 MB input. Here:
   memory;
 * batches take the queue in arrival order; the scheduler sets each
   request's chunk length from its predicted density (cost_model.chunk_for:
-  a unit's serial time bounds a batch's latency, so dense requests get short
-  chunks and sparse ones long chunks) and the queue capacity from the
-  densest prediction; "default" uses the engine's fixed chunks, "static" the
-  table rule's prediction, "learned" the MLP's;
+  a unit's serial time bounds a batch's latency, so requests predicted
+  denser than rho_ref get proportionally shorter chunks, never longer than
+  chunk_hi) and the queue capacity from the densest prediction; "default"
+  uses the engine's fixed chunks, "static" the table rule's prediction,
+  "learned" the MLP's;
 * each request's reports are exactly those of matching it alone
   (test_gpu_serving checks this).
 """
@@ -126,7 +127,7 @@ class Server:
 
     def __init__(self, tableset, predictor=None, rho_ref=2.0, slots=2, budget=1 << 30,
                  max_batch_bytes=64 << 20, device=0, queue_capacity=0,
-                 algorithm="nonblockingpcgroups", base_chunk=2048):
+                 algorithm="nonblockingpcgroups", base_chunk=2048, chunk_lo=256, chunk_hi=2048):
         import torch
         from .engine import Engine
         self.torch = torch
@@ -134,6 +135,7 @@ class Server:
         self.pred = predictor
         self.rho_ref = rho_ref
         self.base_chunk = base_chunk
+        self.chunk_lo, self.chunk_hi = chunk_lo, chunk_hi
         self.budget = budget
         self.max_bytes = max_batch_bytes
         self.queue_capacity = queue_capacity
@@ -144,7 +146,8 @@ class Server:
                        for _ in range(slots)]
         self.rep_cap = max(1 << 16, max_batch_bytes // 4)
         self.busy = [None] * slots      # (batch, event, held bytes, launch arguments)
-        self.batches = []               # (size, bytes, predicted ms, device ms)
+        self.batches = []               # (size, bytes, predicted work, device ms)
+        self.launches = 0               # kernels launched by the served batches
 
     def _held(self):
         return sum(b[2] for b in self.busy if b is not None)
@@ -185,6 +188,7 @@ class Server:
             batch_match_async(eng, self.ts, self.pinned[slot].numpy()[:pos], offs, lens, nfa, **kw)
             eng.sync()
         dev_ms = sum(eng.times_ms())
+        self.launches += eng.launches()
         reps, sids = batch_results(eng)
         per = split_by_stream(reps, sids, len(batch))
         t = time.perf_counter() - self._t0
@@ -222,7 +226,8 @@ class Server:
                 nxt += 1
             if self.pred is not None and nxt > first:  # predictions at arrival, inside the clock
                 rho = self.pred.density(reqs[first:nxt])
-                chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk)
+                chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk, self.chunk_lo,
+                                      self.chunk_hi)
                 for r, d, c in zip(reqs[first:nxt], rho, chunks):
                     r.pred_work = float(d) * len(r.data)
                     r.chunk = int(c)
