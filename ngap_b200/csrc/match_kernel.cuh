@@ -145,6 +145,7 @@ struct TileView {
   int cw;
   int narrow;
   uint32_t nlive;  // live classes: base of the prefix-table keys
+  uint32_t rep_levels;  // bit d: the depth-(d+1) table has report lists
 };
 
 // Successors of v in the 32-bit convention (bit 31 = report, kNoSucc = none).
@@ -487,23 +488,29 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
   // first d symbols remain and no state needs expanding
   const int kmax = valid ? min(depth, c.wlen - r) : 0;
   int k = kmax;
-  for (int d = 0; d < depth; d++)
-    if (d < k && c.in[r + d] >= tv.nlive) k = d;
-  const bool keep_states = k == kmax;
-  uint32_t key = 0, vb = 0, ve = 0;
+  uint32_t key = 0;  // live classes of the next k symbols, base nlive
   for (int d = 0; d < depth; d++) {
-    const bool act = d < k;
-    if (act) key = key * tv.nlive + c.in[r + d];
-    const PrefixTableDev& pt = tv.pt[d];
-    const bool want_v = act && keep_states && d == k - 1;
-    const bool want_r = act && pt.has_reports;
-    uint32_t b0, e0, rb, re;
-    pt_find(pt, key, want_v, want_r, b0, e0, rb, re);
-    if (want_v) {
-      vb = b0;
-      ve = e0;
+    if (d < k) {
+      const uint32_t sym = c.in[r + d];
+      if (sym >= tv.nlive) k = d;
+      else key = key * tv.nlive + sym;
     }
-    if (pt.has_reports) {
+  }
+  const bool keep_states = k == kmax;
+  uint32_t vb = 0, ve = 0;
+  if (keep_states && k > 0) {  // one lookup: the deepest table the lane can use
+    uint32_t rb, re;
+    pt_find(tv.pt[k - 1], key, true, false, vb, ve, rb, re);
+  }
+  if (tv.rep_levels) {  // reports of the first k symbols, level by level
+    uint32_t kk = 0;
+    for (int d = 0; d < depth; d++) {
+      const bool act = d < k;
+      if (act) kk = kk * tv.nlive + c.in[r + d];
+      if (!((tv.rep_levels >> d) & 1u)) continue;
+      const PrefixTableDev& pt = tv.pt[d];
+      uint32_t b0, e0, rb, re;
+      pt_find(pt, kk, false, act, b0, e0, rb, re);
       const int len = (int)(re - rb);
       const int mx = __reduce_max_sync(kFull, len);
       for (int i = 0; i < mx; i++) {
@@ -952,6 +959,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     tv.cw = t->cw;
     tv.narrow = t->narrow;
     tv.nlive = (uint32_t)t->nlive;
+    tv.rep_levels = 0u;
+    for (int d = 0; d < kMaxDepth; d++) tv.rep_levels |= (s_pt[d].has_reports ? 1u : 0u) << d;
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
     const bool translate = t->cw != 8;
