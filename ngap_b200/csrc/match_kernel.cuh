@@ -531,6 +531,28 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
   }
   const uint32_t total = __shfl_sync(kFull, incl, 31);
   if (total == 0) return;
+  if (__reduce_max_sync(kFull, len) <= 4u) {
+    // short lists (the usual case with deep tables): every lane copies its own
+    const int kk = k > 0 ? k : 1;
+    const uint32_t off = (uint32_t)(r + kk - 1);
+    const uint32_t* vl = tv.pt[kk - 1].vlist;
+    for (uint32_t j = 0; j < len; j++) {
+      const uint32_t v = __ldg(vl + vb + j);
+      uint32_t e = (v << kEntryPosBits) | off;
+      if (tv.sticky && is_sticky(tv, v)) {  // registered after the copy instead
+        const uint32_t slot = atomicAdd(ws.pend_n, 1u);
+        if (slot < (uint32_t)kPendCap) {
+          ws.pend_s[slot] = v;
+          ws.pend_q[slot] = (uint32_t)(c.wb + off);
+          e = kNoEntry;
+        }
+      }
+      store_entry(p, ws, w, w.top + (int)(incl - len + j), e);
+    }
+    grow_stack(p, w, (int)total);
+    __syncwarp();
+    return;
+  }
   ws.inj[lane] = incl;
   ws.inj[32 + lane] = vb;
   ws.inj[64 + lane] = (uint32_t)(k > 0 ? k : 1);
