@@ -36,7 +36,7 @@
 
 namespace ngap {
 
-constexpr int kWarpsPerCta = 16;
+constexpr int kWarpsPerCta = 20;
 constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr int kStackCap = 512;    // entries per warp in shared memory
 constexpr int kReportBuf = 64;    // reports per warp buffered in shared memory
