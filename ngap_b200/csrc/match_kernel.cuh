@@ -15,7 +15,7 @@
 // B200 organisation (not the reference's):
 //  * a CTA takes a task (a tile and a range of its units) and stages the
 //    tile's table image (successors, byte-class masks, report bits, byte ->
-//    class map) into shared memory once; its 16 warps then take units of that
+//    class map) into shared memory once; its warps (kWarpsPerCta) then take units of that
 //    task, one warp per unit, with no block-wide barrier in the hot loop;
 //  * per warp, in shared memory: a LIFO worklist of packed entries
 //    (state << 13 | offset in the window); one expansion step pops up to 32
