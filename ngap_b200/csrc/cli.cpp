@@ -163,6 +163,7 @@ bool parse_args(int argc, char** argv, Options& o, std::string& err) {
       return false;
     }
   }
+  if (o.show_help) return true;  // help needs no input
   if (o.input_filename.empty()) {
     err = "Option --input is required";
     return false;
@@ -223,7 +224,10 @@ int main(int argc, char** argv) {
     std::cerr << "Error in command line: " << perr << std::endl;
     return 1;
   }
-  if (o.show_help) print_help();
+  if (o.show_help) {
+    print_help();
+    return 0;
+  }
 
   // input stream (SymbolStream::readFromFile + slice, main.cu:45-50)
   std::ifstream f(o.input_filename, std::ios::binary);
