@@ -188,7 +188,8 @@ typedef struct ngap_unit_trace {
   uint64_t work;    /* worklist entries the unit expanded plus entries it injected */
 } ngap_unit_trace;
 int ngap_engine_set_trace(ngap_engine* e, int enable);
-/* Copies the last match's unit records (after ngap_engine_sync); *n = count. */
+/* Copies up to cap of the last match's unit records (after ngap_engine_sync);
+ * *n = records copied, or with out = NULL the number of records. */
 int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* n);
 
 /* Statistics of built tables, the NFA features of the cost model. The

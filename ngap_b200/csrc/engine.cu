@@ -1168,12 +1168,16 @@ int ngap_engine_set_trace(ngap_engine* e, int enable) {
 }
 
 int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* n) {
-  if (!e || !n || (!out && cap > 0)) {
+  if (!e || !n) {
     set_error("ngap_trace_copy: bad argument");
     return NGAP_E_INVALID;
   }
   *n = 0;
   if (!e->trace || !e->ran || e->nunits == 0 || !e->d_unit_work) return NGAP_OK;
+  if (!out) {  // count query
+    *n = e->nunits;
+    return NGAP_OK;
+  }
   std::vector<unsigned long long> work(e->nunits);
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));

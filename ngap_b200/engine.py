@@ -189,7 +189,8 @@ class Engine:
         fields stream, tile, lo, hi (positions relative to the segment or
         stream) and work (entries expanded + injected)."""
         n = ctypes.c_int64()
-        cap = 1 << 22
+        check(lib().ngap_trace_copy(self._h, None, 0, ctypes.byref(n)))
+        cap = max(1, n.value)
         buf = (_lib.UnitTrace * cap)()
         check(lib().ngap_trace_copy(self._h, buf, cap, ctypes.byref(n)))
         dt = np.dtype([("stream", np.int32), ("tile", np.int32), ("lo", np.int64),
