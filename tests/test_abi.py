@@ -1,5 +1,6 @@
 """The C-ABI library (CPU): loads, exports every declared symbol, and its
 host-only entry points work without a GPU. Also the CLI's argument handling."""
+import ctypes
 import os
 import re
 import subprocess
@@ -68,3 +69,22 @@ def test_cli_unknown_algorithm(tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 0
     assert "not supported algoritm nosuch" in r.stdout and "FINISHED!" in r.stdout
+
+
+def test_scheduler_entry_points_reject_bad_arguments(built):
+    L = nb.lib()
+    assert L.ngap_engine_set_trace(None, 1) == 1
+    assert L.ngap_trace_copy(None, None, 0, None) == 1
+    assert L.ngap_tables_stats_get(None, None) == 1
+    assert L.ngap_features(None, 0, 0, None, None, 1, 1024, None, None) == 1
+    assert L.ngap_mlp_train(None, None, None, 0, 1, 1, ctypes.c_float(0.1), None) == 1
+    assert L.ngap_mlp_predict(None, None, 0, 0, None) == 1
+    assert L.ngap_mlp_set_params(None, None, 0) == 1
+    assert L.ngap_engine_device_bytes(None) == 0
+
+
+def test_cli_help_and_new_flags():
+    r = subprocess.run([CLI, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--tile-mode" in r.stdout and "usage: ngap" in r.stdout
+    r = subprocess.run([CLI, "--tile-mode", "x"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unable to convert" in r.stderr
