@@ -20,9 +20,9 @@ from the longest prefix-table list (kernel_ngap_OA.cu:180-194). Here:
   baseline: the mean traced density of each NFA. LearnedModel is the 2 x 64
   MLP of ngap_mlp_* (FP32 training, BF16 or FP32 inference) on the log of the
   density;
-* plan() turns per-stream predictions into per-stream chunk lengths (about
-  the same predicted work per unit) and a queue capacity. Neither changes any
-  report: they only reshape the work.
+* chunk_for / plan turn per-stream predictions into per-stream chunk lengths
+  (shorter for denser streams) and queue_for into a queue capacity. Neither
+  changes any report: they only reshape the work.
 """
 import ctypes
 import math

@@ -11,9 +11,9 @@ single 1 MB input. Here:
   from the queued requests and launches it with ngap_batch_match, so that
   requests arriving while others run are admitted as slots and memory free
   up, and batches on different slots overlap on the device;
-* admission: a batch is launched only while the bytes held by in-flight
-  batches (input plus report capacity) stay within `budget` bytes of device
-  memory;
+* admission: a batch is launched only while the input bytes held by
+  in-flight batches stay within `budget` bytes of device memory (each
+  engine's report buffers are sized once, for `max_batch_bytes`);
 * batches take the queue in arrival order; the scheduler sets each
   request's chunk length from its predicted density (cost_model.chunk_for:
   a unit's serial time bounds a batch's latency, so requests predicted
@@ -22,7 +22,7 @@ single 1 MB input. Here:
   uses the engine's fixed chunks, "static" the table rule's prediction,
   "learned" the MLP's;
 * each request's reports are exactly those of matching it alone
-  (test_gpu_serving checks this).
+  (tests/test_gpu_cost_model.py checks this for every scheduler).
 """
 import math
 import time
