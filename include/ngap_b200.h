@@ -124,6 +124,27 @@ typedef struct ngap_table_opts {
  * (code/src/ngap/ngap.cu:3086-3111, prefix tables ngap.cu:2358-2513). */
 int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_tables** out);
 void ngap_tables_destroy(ngap_tables* t);
+/* The tiles ngap_tables_build would make, planned on the host only (no
+ * device memory, no GPU needed): one record per tile, at most cap; *n = tile
+ * count. The reference has no tiles (its unit of work is a whole group,
+ * code/src/ngap/ngap.cu:1507); this exposes the partition for inspection. */
+typedef struct ngap_tile_desc {
+  int32_t phase;      /* 0 plain, 1 activation (dot-star CCs), 2 layered */
+  int32_t pair;       /* activation/layered pair index, -1 for plain tiles */
+  int32_t group;      /* group of the tile's first CC */
+  int32_t num_states, num_ccs;
+  int32_t nact;       /* sticky states of the pair (activation slots) */
+  int32_t nsticky;    /* sticky states handled in the tile */
+  int32_t global;     /* 1: tables read through L2 (several groups possible) */
+  int32_t depth;      /* prefix-table depth */
+  int32_t max_path;   /* longest acyclic path (chunk warm-up + 1); -1 = cyclic */
+  int32_t nlive;      /* live byte classes */
+  int32_t pad;
+  int64_t table_bytes; /* prefix tables and image */
+} ngap_tile_desc;
+int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
+                        int cap, int* n);
+
 /* Bytes of device memory held by the tables. */
 int64_t ngap_tables_device_bytes(const ngap_tables* t);
 

@@ -54,6 +54,12 @@ class TableOpts(ctypes.Structure):
                 ("max_table_entries", ctypes.c_int64), ("tile_mode", ctypes.c_int)]
 
 
+class TileDesc(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in (
+        "phase", "pair", "group", "num_states", "num_ccs", "nact", "nsticky", "global_",
+        "depth", "max_path", "nlive", "pad")] + [("table_bytes", ctypes.c_int64)]
+
+
 class MatchParams(ctypes.Structure):
     _fields_ = [("algorithm", ctypes.c_int), ("num_seg", ctypes.c_int64),
                 ("seg_len", ctypes.c_int64), ("is_dup", ctypes.c_int), ("unique", ctypes.c_int),
@@ -110,6 +116,9 @@ SIGNATURES = {
     "ngap_tables_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableOpts),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "ngap_tables_destroy": (None, [ctypes.c_void_p]),
+    "ngap_tiles_describe": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableOpts),
+                                           ctypes.POINTER(TileDesc), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int)]),
     "ngap_tables_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
     "ngap_engine_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "ngap_engine_destroy": (None, [ctypes.c_void_p]),

@@ -10,6 +10,7 @@
 
 #include "common.h"
 #include "handles.h"
+#include "tables.h"
 
 namespace ngap {
 
@@ -131,6 +132,58 @@ int ngap_group_view_get(const ngap_groups* g, int group, ngap_group_view* out) {
 }
 
 void ngap_groups_destroy(ngap_groups* g) { delete g; }
+
+int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
+                        int cap, int* n) {
+  if (!g || !n || (cap > 0 && !out)) {
+    set_error("ngap_tiles_describe: null argument");
+    return NGAP_E_INVALID;
+  }
+  *n = 0;
+  ngap_table_opts o{};
+  o.precompute_cutoff = -1;
+  if (opts) o = *opts;
+  if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth ||
+      o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
+    set_error("ngap_tiles_describe: precompute_depth must be in -1..%d and tile_mode 0..2",
+              kMaxDepth);
+    return NGAP_E_INVALID;
+  }
+  TableOpts to;
+  to.precompute_depth = o.precompute_depth;
+  to.precompute_cutoff = o.precompute_cutoff;
+  to.tile_states = o.tile_states;
+  to.max_table_entries = o.max_table_entries;
+  to.tile_mode = o.tile_mode;
+  std::vector<TileHost> tiles;
+  const int rc = build_tiles(g->gs, to, tiles);
+  if (rc != NGAP_OK) return rc;
+  *n = (int)tiles.size();
+  for (int i = 0; i < std::min(cap, (int)tiles.size()); i++) {
+    const TileHost& t = tiles[i];
+    ngap_tile_desc d{};
+    d.phase = t.phase;
+    d.pair = t.pair;
+    d.group = t.group;
+    d.num_states = t.nstates;
+    d.num_ccs = t.num_ccs;
+    d.nact = t.nact;
+    d.nsticky = t.nsticky;
+    d.global = t.global ? 1 : 0;
+    d.depth = t.depth;
+    d.max_path = t.max_path;
+    d.nlive = t.nlive;
+    int64_t b = (int64_t)t.image.size();
+    for (int k = 0; k < t.depth; k++) {
+      const PrefixTableHost& p = t.pt[k];
+      b += 4 * (int64_t)(p.voff.size() + p.roff.size() + p.slots.size() + p.vlist.size() +
+                         p.rlist.size());
+    }
+    d.table_bytes = b;
+    out[i] = d;
+  }
+  return NGAP_OK;
+}
 
 // The reference validates with a CPU frontier simulation (ngap.cu:2171-2268)
 // and a sort/unique comparison (ngap.cu:2270-2344). This checker does the same

@@ -108,6 +108,25 @@ class Groups:
     def views(self):
         return [self.view(g) for g in range(self.count)]
 
+    def tiles(self, precompute_depth=0, tile_states=0, tile_mode="auto", max_table_entries=0):
+        """The tiles Tables(...) would build, planned on the host (no GPU):
+        list of dicts (phase, pair, group, num_states, num_ccs, nact, nsticky,
+        global, depth, max_path, nlive, table_bytes)."""
+        modes = {"auto": 0, "shared": 1, "global": 2}
+        opts = _lib.TableOpts(0, precompute_depth, -1, tile_states, max_table_entries,
+                              modes[tile_mode])
+        n = ctypes.c_int()
+        check(lib().ngap_tiles_describe(self._h, ctypes.byref(opts), None, 0, ctypes.byref(n)))
+        buf = (_lib.TileDesc * max(1, n.value))()
+        check(lib().ngap_tiles_describe(self._h, ctypes.byref(opts), buf, n.value,
+                                        ctypes.byref(n)))
+        out = []
+        for d in buf[:n.value]:
+            r = {k: getattr(d, k) for k, _ in _lib.TileDesc._fields_ if k != "pad"}
+            r["global"] = r.pop("global_")
+            out.append(r)
+        return out
+
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:
             _lib._lib.ngap_groups_destroy(self._h)

@@ -81,6 +81,12 @@ def test_scheduler_entry_points_reject_bad_arguments(built):
     assert L.ngap_mlp_predict(None, None, 0, 0, None) == 1
     assert L.ngap_mlp_set_params(None, None, 0) == 1
     assert L.ngap_engine_device_bytes(None) == 0
+    n = ctypes.c_int(-5)
+    assert L.ngap_tiles_describe(None, None, None, 0, ctypes.byref(n)) == 1
+    g = nb.Groups(nb.Nfa.from_string(open(os.path.join(ROOT, "tests", "golden",
+                                                       "apple.anml")).read()), group_num=1)
+    assert L.ngap_tiles_describe(g._h, None, None, 4, ctypes.byref(n)) == 1  # cap > 0, no out
+    assert L.ngap_tiles_describe(g._h, None, None, 0, ctypes.byref(n)) == 0 and n.value == 1
 
 
 def test_cli_help_and_new_flags():
