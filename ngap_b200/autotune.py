@@ -10,7 +10,6 @@ are represented) and the fastest one is kept; results do not depend on the
 choice.
 """
 import itertools
-import time
 
 import numpy as np
 
@@ -23,15 +22,17 @@ DEFAULT_GRID = {
 }
 
 
-def sample_streams(offsets, lengths, nfa_of, frac=0.05, seed=0, min_streams=32):
-    """Indices of a byte-weighted random sample of whole streams."""
+def sample_streams(lengths, frac=0.05, seed=0, min_streams=32):
+    """Sorted indices of a random sample of whole streams: streams in a seeded
+    random order until they hold `frac` of the bytes and number at least
+    min_streams (or all of them)."""
     rng = np.random.default_rng(seed)
-    order = rng.permutation(len(offsets))
+    order = rng.permutation(len(lengths))
     total, budget, pick = 0, max(1, int(frac * int(np.sum(lengths)))), []
     for i in order:
         pick.append(int(i))
         total += int(lengths[i])
-        if total >= budget and len(pick) >= min(min_streams, len(offsets)):
+        if total >= budget and len(pick) >= min(min_streams, len(lengths)):
             break
     return np.array(sorted(pick), dtype=np.int64)
 
@@ -40,7 +41,7 @@ def autotune(engine, tableset, data, offsets, lengths, nfa_of, grid=None, frac=0
              stream=None):
     """Returns (best_params, table of (params, ms)) for batched matching."""
     grid = grid or DEFAULT_GRID
-    idx = sample_streams(offsets, lengths, nfa_of, frac)
+    idx = sample_streams(lengths, frac)
     # compact the sample into its own buffer
     lens = lengths[idx]
     offs = np.zeros(len(idx), dtype=np.int64)
@@ -54,14 +55,12 @@ def autotune(engine, tableset, data, offsets, lengths, nfa_of, grid=None, frac=0
         params = dict(zip(keys, combo))
         best = None
         for r in range(reps + 1):
-            t0 = time.perf_counter()
             batch_match_async(engine, tableset, buf, offs, lens, nf, stream=stream, **params)
             engine.sync()
             ms = engine.times_ms()
             dev = ms[0] + ms[1]
             if r > 0:  # first run warms the plan and buffers
                 best = dev if best is None else min(best, dev)
-            del t0
         results.append((params, best))
     results.sort(key=lambda x: x[1])
     return results[0][0], results

@@ -65,3 +65,34 @@ def test_poisson_requests():
     assert 1800 < len(reqs) < 2200 and np.all(np.diff(t) > 0) and t[-1] < 1.0
     assert 50000 < np.median(L) < 80000
     assert set(r.nfa for r in reqs) == {0, 1, 2}
+
+
+def test_autotune_sample_streams():
+    from ngap_b200 import autotune as at
+    lengths = np.arange(1, 201, dtype=np.int64) * 100
+    idx = at.sample_streams(lengths, frac=0.05, min_streams=8)
+    assert np.all(np.diff(idx) > 0) and len(idx) >= 8
+    assert lengths[idx].sum() >= 0.05 * lengths.sum()
+    assert np.array_equal(idx, at.sample_streams(lengths, frac=0.05, min_streams=8))
+    assert len(at.sample_streams(lengths[:5], frac=0.01, min_streams=32)) == 5
+    assert len(at.sample_streams(lengths, frac=1.0)) == 200
+
+
+def _server(budget, max_bytes, held=()):
+    s = sv.Server.__new__(sv.Server)  # the admission rule only: no engines or streams
+    s.budget, s.max_bytes = budget, max_bytes
+    s.busy = [(None, None, h, None) for h in held] + [None]
+    return s
+
+
+def test_serving_admission():
+    reqs = [sv.Request(i, 0, np.zeros(n, np.uint8), 0.0) for i, n in enumerate([40, 30, 20, 50])]
+    q = list(reqs)
+    s = _server(budget=1000, max_bytes=90)  # batch capped by max_batch_bytes, in arrival order
+    assert [r.rid for r in s._form(q)] == [0, 1, 2] and [r.rid for r in q] == [3]
+    q = list(reqs)
+    s = _server(budget=100, max_bytes=1000, held=(35,))  # 65 bytes free under the budget
+    assert [r.rid for r in s._form(q)] == [0] and len(q) == 3
+    q = list(reqs)
+    s = _server(budget=100, max_bytes=1000, held=(80,))  # the first request does not fit: none
+    assert s._form(q) == [] and len(q) == 4
