@@ -339,7 +339,7 @@ int ngap_features(const uint8_t* data, uint64_t bytes, int on_device, const uint
     return NGAP_E_INVALID;
   }
   for (int i = 0; i < n; i++)
-    if (offsets[i] + lengths[i] > bytes) {
+    if (offsets[i] > bytes || lengths[i] > bytes - offsets[i]) {  // no wrap-around
       ngap::set_error("ngap_features: region %d is out of range", i);
       return NGAP_E_INVALID;
     }

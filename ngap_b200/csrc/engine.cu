@@ -911,7 +911,7 @@ extern "C" {
 
 int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int input_on_device,
                const ngap_match_params* p, void* stream) {
-  if (!e || !t || !p || (!input && p->num_seg * p->seg_len > 0)) {
+  if (!e || !t || !p) {
     set_error("ngap_match: null argument");
     return NGAP_E_INVALID;
   }
@@ -919,7 +919,14 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     set_error("ngap_match: num_seg and seg_len must be positive");
     return NGAP_E_INVALID;
   }
-  const uint64_t total = (uint64_t)p->num_seg * (uint64_t)p->seg_len;
+  if (!input) {
+    set_error("ngap_match: null argument (input)");
+    return NGAP_E_INVALID;
+  }
+  // each factor below 2^32 first, so that the product cannot wrap
+  const uint64_t total = p->num_seg < (1ll << 32) && p->seg_len < (1ll << 32)
+                             ? (uint64_t)p->num_seg * (uint64_t)p->seg_len
+                             : ~0ull;
   if (total >= (1ull << 32)) {
     set_error("ngap_match: input of %llu bytes exceeds the 32-bit offsets of the report format",
               (unsigned long long)total);
@@ -1323,7 +1330,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   uint64_t max_len = 1;
   for (int i = 0; i < nstreams; i++) {
     const ngap_batch_stream& s = streams[i];
-    if (s.nfa < 0 || s.nfa >= (int)ts->tables.size() || s.offset + s.length > input_bytes) {
+    if (s.nfa < 0 || s.nfa >= (int)ts->tables.size() || s.offset > input_bytes ||
+        s.length > input_bytes - s.offset) {  // no wrap-around of offset + length
       set_error("ngap_batch_match: stream %d is out of range", i);
       return NGAP_E_INVALID;
     }

@@ -77,6 +77,12 @@ def test_scheduler_entry_points_reject_bad_arguments(built):
     assert L.ngap_trace_copy(None, None, 0, None) == 1
     assert L.ngap_tables_stats_get(None, None) == 1
     assert L.ngap_features(None, 0, 0, None, None, 1, 1024, None, None) == 1
+    # a region whose offset + length wraps past 2^64 is out of range, not accepted
+    data = (ctypes.c_uint8 * 16)()
+    offs, lens = (ctypes.c_uint64 * 1)(2**64 - 1), (ctypes.c_uint64 * 1)(2)
+    out = (ctypes.c_float * _lib.FEAT_BYTES)()
+    assert L.ngap_features(data, 16, 0, offs, lens, 1, 1024, out, None) == 1
+    assert "out of range" in _lib.last_error()
     assert L.ngap_mlp_train(None, None, None, 0, 1, 1, ctypes.c_float(0.1), None) == 1
     assert L.ngap_mlp_predict(None, None, 0, 0, None) == 1
     assert L.ngap_mlp_set_params(None, None, 0) == 1
