@@ -139,11 +139,27 @@ typedef struct ngap_tile_desc {
   int32_t depth;      /* prefix-table depth */
   int32_t max_path;   /* longest acyclic path (chunk warm-up + 1); -1 = cyclic */
   int32_t nlive;      /* live byte classes */
-  int32_t pad;
+  int32_t dense_levels; /* bit d-1 set: table d is dense (offsets by key), else hashed */
   int64_t table_bytes; /* prefix tables and image */
 } ngap_tile_desc;
 int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
                         int cap, int* n);
+
+/* Host-only check of the prefix tables (no GPU): plans the tiles as
+ * ngap_tiles_describe does, then looks up nkeys byte strings of len bytes
+ * each (keys: nkeys * len bytes; 1 <= len <= the tile's depth) in table len
+ * of tile `tile` the way the matching kernel does (byte -> class -> base-L
+ * key; dense offsets or hash slots). Table d of the reference maps d symbols
+ * to the states reached after them from the always-active states
+ * (code/src/ngap/ngap.cu:2358-2468, precompute_table.h:8-101). For key k,
+ * ids[off[k] .. off[k+1]) are the report ids (group-local sid | group << 22)
+ * of the listed states and reports[roff[k] .. roff[k+1]) those of its report
+ * states; off and roff hold nkeys + 1 entries and ids and reports room for
+ * cap entries each. When cap is too small the call returns NGAP_E_INVALID
+ * with off[nkeys] and roff[nkeys] set to the entries needed. */
+int ngap_tiles_lookup(const ngap_groups* g, const ngap_table_opts* opts, int tile,
+                      const uint8_t* keys, int nkeys, int len, uint32_t* ids, int64_t* off,
+                      uint32_t* reports, int64_t* roff, int64_t cap);
 
 /* Bytes of device memory held by the tables. */
 int64_t ngap_tables_device_bytes(const ngap_tables* t);

@@ -57,7 +57,7 @@ class TableOpts(ctypes.Structure):
 class TileDesc(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in (
         "phase", "pair", "group", "num_states", "num_ccs", "nact", "nsticky", "global_",
-        "depth", "max_path", "nlive", "pad")] + [("table_bytes", ctypes.c_int64)]
+        "depth", "max_path", "nlive", "dense_levels")] + [("table_bytes", ctypes.c_int64)]
 
 
 class MatchParams(ctypes.Structure):
@@ -116,6 +116,10 @@ SIGNATURES = {
     "ngap_tables_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableOpts),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "ngap_tables_destroy": (None, [ctypes.c_void_p]),
+    "ngap_tiles_lookup": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableOpts), ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_int64]),
     "ngap_tiles_describe": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableOpts),
                                            ctypes.POINTER(TileDesc), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_int)]),

@@ -133,20 +133,17 @@ int ngap_group_view_get(const ngap_groups* g, int group, ngap_group_view* out) {
 
 void ngap_groups_destroy(ngap_groups* g) { delete g; }
 
-int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
-                        int cap, int* n) {
-  if (!g || !n || (cap > 0 && !out)) {
-    set_error("ngap_tiles_describe: null argument");
-    return NGAP_E_INVALID;
-  }
-  *n = 0;
+namespace {
+
+// The tiles ngap_tables_build would make, planned on the host.
+int plan_tiles(const char* fn, const ngap_groups* g, const ngap_table_opts* opts,
+               std::vector<TileHost>& tiles) {
   ngap_table_opts o{};
   o.precompute_cutoff = -1;
   if (opts) o = *opts;
   if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth ||
       o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
-    set_error("ngap_tiles_describe: precompute_depth must be in -1..%d and tile_mode 0..2",
-              kMaxDepth);
+    set_error("%s: precompute_depth must be in -1..%d and tile_mode 0..2", fn, kMaxDepth);
     return NGAP_E_INVALID;
   }
   TableOpts to;
@@ -155,8 +152,50 @@ int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_
   to.tile_states = o.tile_states;
   to.max_table_entries = o.max_table_entries;
   to.tile_mode = o.tile_mode;
+  return build_tiles(g->gs, to, tiles);
+}
+
+// [vb, ve) and [rb, re) of `key` in a prefix table, laid out as the matching
+// kernel reads it (dense offsets by key, or linear-probing hash slots
+// {key, list begin, report-list begin, list length << 16 | report length}).
+void table_find(const PrefixTableHost& t, uint32_t key, uint32_t& vb, uint32_t& ve, uint32_t& rb,
+                uint32_t& re) {
+  vb = ve = rb = re = 0;
+  if (t.dense) {
+    vb = t.voff[key];
+    ve = t.voff[key + 1];
+    if (!t.roff.empty()) {
+      rb = t.roff[key];
+      re = t.roff[key + 1];
+    }
+    return;
+  }
+  uint32_t h = prefix_hash(key) & t.hmask;
+  for (uint32_t probe = 0; probe <= t.hmask; probe++) {
+    const uint32_t* s = &t.slots[(size_t)h * 4];
+    if (s[0] == key) {
+      vb = s[1];
+      ve = s[1] + (s[3] >> 16);
+      rb = s[2];
+      re = s[2] + (s[3] & 0xffffu);
+      return;
+    }
+    if (s[0] == kHashEmpty) return;
+    h = (h + 1) & t.hmask;
+  }
+}
+
+}  // namespace
+
+int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
+                        int cap, int* n) {
+  if (!g || !n || (cap > 0 && !out)) {
+    set_error("ngap_tiles_describe: null argument");
+    return NGAP_E_INVALID;
+  }
+  *n = 0;
   std::vector<TileHost> tiles;
-  const int rc = build_tiles(g->gs, to, tiles);
+  const int rc = plan_tiles("ngap_tiles_describe", g, opts, tiles);
   if (rc != NGAP_OK) return rc;
   *n = (int)tiles.size();
   for (int i = 0; i < std::min(cap, (int)tiles.size()); i++) {
@@ -178,9 +217,57 @@ int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_
       const PrefixTableHost& p = t.pt[k];
       b += 4 * (int64_t)(p.voff.size() + p.roff.size() + p.slots.size() + p.vlist.size() +
                          p.rlist.size());
+      if (p.dense) d.dense_levels |= 1 << k;
     }
     d.table_bytes = b;
     out[i] = d;
+  }
+  return NGAP_OK;
+}
+
+int ngap_tiles_lookup(const ngap_groups* g, const ngap_table_opts* opts, int tile,
+                      const uint8_t* keys, int nkeys, int len, uint32_t* ids, int64_t* off,
+                      uint32_t* reports, int64_t* roff, int64_t cap) {
+  if (!g || nkeys < 0 || !off || !roff || (nkeys > 0 && !keys) || (cap > 0 && (!ids || !reports))) {
+    set_error("ngap_tiles_lookup: null argument");
+    return NGAP_E_INVALID;
+  }
+  std::vector<TileHost> tiles;
+  const int rc = plan_tiles("ngap_tiles_lookup", g, opts, tiles);
+  if (rc != NGAP_OK) return rc;
+  if (tile < 0 || tile >= (int)tiles.size()) {
+    set_error("ngap_tiles_lookup: tile %d of %d", tile, (int)tiles.size());
+    return NGAP_E_INVALID;
+  }
+  const TileHost& t = tiles[tile];
+  if (len < 1 || len > t.depth) {
+    set_error("ngap_tiles_lookup: len must be in 1..%d (the tile's depth)", t.depth);
+    return NGAP_E_INVALID;
+  }
+  const PrefixTableHost& pt = t.pt[len - 1];
+  const uint32_t L = (uint32_t)t.nlive;
+  int64_t nv = 0, nr = 0;
+  off[0] = roff[0] = 0;
+  for (int k = 0; k < nkeys; k++) {
+    uint32_t key = 0, vb = 0, ve = 0, rb = 0, re = 0;
+    bool dead = false;
+    for (int i = 0; i < len; i++) {
+      const uint32_t c = t.cls[keys[(size_t)k * len + i]];
+      dead = dead || c >= L;  // a dead byte ends every path: no lookup
+      key = key * L + c;
+    }
+    if (!dead) table_find(pt, key, vb, ve, rb, re);
+    for (uint32_t j = vb; j < ve; j++, nv++)
+      if (nv < cap) ids[nv] = t.sid[pt.vlist[j]];
+    for (uint32_t j = rb; j < re; j++, nr++)
+      if (nr < cap) reports[nr] = t.sid[pt.rlist[j]];
+    off[k + 1] = nv;
+    roff[k + 1] = nr;
+  }
+  if (nv > cap || nr > cap) {
+    set_error("ngap_tiles_lookup: %lld states and %lld reports, room for %lld", (long long)nv,
+              (long long)nr, (long long)cap);
+    return NGAP_E_INVALID;
   }
   return NGAP_OK;
 }

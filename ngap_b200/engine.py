@@ -108,13 +108,19 @@ class Groups:
     def views(self):
         return [self.view(g) for g in range(self.count)]
 
+    @staticmethod
+    def _plan_opts(precompute_depth, tile_states, tile_mode, max_table_entries):
+        modes = {"auto": 0, "shared": 1, "global": 2}
+        if tile_mode not in modes:
+            raise ValueError(f"tile_mode must be one of {sorted(modes)}")
+        return _lib.TableOpts(0, precompute_depth, -1, tile_states, max_table_entries,
+                              modes[tile_mode])
+
     def tiles(self, precompute_depth=0, tile_states=0, tile_mode="auto", max_table_entries=0):
         """The tiles Tables(...) would build, planned on the host (no GPU):
         list of dicts (phase, pair, group, num_states, num_ccs, nact, nsticky,
-        global, depth, max_path, nlive, table_bytes)."""
-        modes = {"auto": 0, "shared": 1, "global": 2}
-        opts = _lib.TableOpts(0, precompute_depth, -1, tile_states, max_table_entries,
-                              modes[tile_mode])
+        global, depth, max_path, nlive, dense_levels, table_bytes)."""
+        opts = self._plan_opts(precompute_depth, tile_states, tile_mode, max_table_entries)
         n = ctypes.c_int()
         check(lib().ngap_tiles_describe(self._h, ctypes.byref(opts), None, 0, ctypes.byref(n)))
         buf = (_lib.TileDesc * max(1, n.value))()
@@ -122,10 +128,38 @@ class Groups:
                                         ctypes.byref(n)))
         out = []
         for d in buf[:n.value]:
-            r = {k: getattr(d, k) for k, _ in _lib.TileDesc._fields_ if k != "pad"}
+            r = {k: getattr(d, k) for k, _ in _lib.TileDesc._fields_}
             r["global"] = r.pop("global_")
             out.append(r)
         return out
+
+    def table_lookup(self, tile, keys, precompute_depth=0, tile_states=0, tile_mode="auto",
+                     max_table_entries=0):
+        """Looks up byte strings (uint8 array [n, d]) in prefix table d of a
+        tile, planned on the host as tiles() plans it. Returns, per string,
+        (ids, report_ids): the report ids (sid | group << 22) of the states
+        the table lists and of its report states."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint8)
+        if keys.ndim != 2:
+            raise ValueError("keys must be a 2-D uint8 array [n, length]")
+        opts = self._plan_opts(precompute_depth, tile_states, tile_mode, max_table_entries)
+        n, d = keys.shape
+        off = np.zeros(n + 1, np.int64)
+        roff = np.zeros(n + 1, np.int64)
+        cap = max(1024, 4 * n)
+        while True:
+            ids = np.zeros(cap, np.uint32)
+            reps = np.zeros(cap, np.uint32)
+            rc = lib().ngap_tiles_lookup(self._h, ctypes.byref(opts), tile, keys.ctypes.data, n, d,
+                                         ids.ctypes.data, off.ctypes.data, reps.ctypes.data,
+                                         roff.ctypes.data, cap)
+            need = max(int(off[n]), int(roff[n]))
+            if rc != 0 and need > cap:
+                cap = need
+                continue
+            check(rc)
+            return [(ids[off[k]:off[k + 1]].copy(), reps[roff[k]:roff[k + 1]].copy())
+                    for k in range(n)]
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value and _lib._lib is not None:

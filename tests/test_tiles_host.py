@@ -88,3 +88,92 @@ def test_bad_options_are_errors():
     with pytest.raises(nb.NgapError):
         g.tiles(precompute_depth=13)
     assert g.tiles(precompute_depth=-1)[0]["depth"] >= 1
+
+
+def _expected_lists(views, groups_of_tile, keys):
+    """Prefix-table semantics restated on the group graphs: table d maps d
+    bytes to the states reached after them, starting from the always-active
+    states that accept the first byte and following successor edges whose
+    target accepts the next byte (edges into always-active states are not
+    followed: those states are injected at every position anyway). Returns
+    per key (sorted ids, sorted report ids), ids = state | group << 22."""
+    out = []
+    for key in keys:
+        ids, reps = set(), set()
+        for gi in groups_of_tile:
+            v = views[gi]
+            bits = np.asarray(v.symbol_sets).reshape(-1, 8)
+            row, col = np.asarray(v.row_offsets), np.asarray(v.col_indices)
+            attrs, aas = np.asarray(v.node_attrs), np.asarray(v.always_active)
+            aas_set = set(aas.tolist())
+            acc = lambda s, b: (int(bits[s, b >> 5]) >> (b & 31)) & 1
+            cur = {int(a) for a in aas if acc(a, int(key[0]))}
+            for b in key[1:]:
+                cur = {int(u) for s in cur for u in col[row[s]:row[s + 1]]
+                       if int(u) not in aas_set and acc(u, int(b))}
+            ids |= {s | gi << 22 for s in cur}
+            reps |= {s | gi << 22 for s in cur if attrs[s] & 2}
+        out.append((sorted(ids), sorted(reps)))
+    return out
+
+
+def _keys(data, rng, depth, n=120, plant_every=1 << 9):
+    """Substrings of the input at the planted matches and at random places
+    (lists mostly non-empty) and random bytes (mostly dead classes), of every
+    length 1..depth."""
+    out = []
+    planted = list(range(plant_every // 2, len(data) - depth, plant_every))
+    for d in range(1, depth + 1):
+        ks = [data[p:p + d] for p in planted]
+        ks += [data[p:p + d] for p in rng.integers(0, len(data) - d, size=n // 2)]
+        ks += [rng.integers(0, 256, size=d, dtype=np.uint8) for _ in range(n // 2)]
+        out.append(np.stack(ks).astype(np.uint8))
+    return out
+
+
+@pytest.mark.parametrize("case", ["hamming", "literal", "levenshtein", "global3"])
+def test_prefix_tables_match_restated_semantics(case):
+    rng = np.random.default_rng(5)
+    if case == "hamming":
+        anml, data = W.hamming_set(seed=2, n_patterns=3, k=8, input_len=1 << 12, plant_every=1 << 9)
+        g, kw = 1, dict(precompute_depth=5, tile_mode="shared")
+    elif case == "literal":  # 95 classes: byte keys (nlive 256), level 3 hashed
+        anml, data = W.literal_set(seed=1, input_len=1 << 12, plant_every=1 << 9)
+        g, kw = 1, dict(precompute_depth=3, tile_mode="shared")
+    elif case == "levenshtein":
+        anml, data = W.levenshtein_set(seed=3, n_patterns=2, k=8, input_len=1 << 12,
+                                       plant_every=1 << 9)
+        g, kw = 1, dict(precompute_depth=4, tile_mode="shared")
+    else:  # one global tile over three groups: ids carry the group bits
+        anml, data = W.hamming_set(seed=4, n_patterns=6, k=8, input_len=1 << 12, plant_every=1 << 9)
+        g, kw = 3, dict(precompute_depth=4, tile_mode="global")
+    groups = _groups(anml, g)
+    tiles = groups.tiles(**kw)
+    views = groups.views()
+    assert len(tiles) == 1 and tiles[0]["num_ccs"] == sum(len(v.cc_begin) - 1 for v in views)
+    t = tiles[0]
+    if case == "literal":
+        assert t["nlive"] == 256 and t["dense_levels"] & 4 == 0  # level 3 is hashed
+    else:
+        assert t["dense_levels"] == (1 << t["depth"]) - 1
+    nonempty = 0
+    for d, keys in enumerate(_keys(np.asarray(data), rng, t["depth"]), start=1):
+        got = groups.table_lookup(0, keys, **kw)
+        want = _expected_lists(views, range(len(views)), keys)
+        for (ids, reps), (wi, wr) in zip(got, want):
+            assert sorted(ids.tolist()) == wi and sorted(reps.tolist()) == wr
+            nonempty += len(wi) > 0
+    assert nonempty > 50
+
+
+def test_table_lookup_arguments():
+    anml, _ = W.literal_set(seed=1, n_patterns=4, input_len=1 << 10, plant_every=1 << 8)
+    g = _groups(anml, 1)
+    depth = g.tiles(precompute_depth=2)[0]["depth"]
+    with pytest.raises(nb.NgapError):
+        g.table_lookup(0, np.zeros((1, depth + 1), np.uint8), precompute_depth=2)
+    with pytest.raises(nb.NgapError):
+        g.table_lookup(5, np.zeros((1, 1), np.uint8), precompute_depth=2)
+    with pytest.raises(ValueError):
+        g.table_lookup(0, np.zeros(3, np.uint8))
+    assert g.table_lookup(0, np.zeros((0, 1), np.uint8), precompute_depth=2) == []
