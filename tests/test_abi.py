@@ -5,8 +5,6 @@ import os
 import re
 import subprocess
 
-import pytest
-
 import ngap_b200 as nb
 from ngap_b200 import _lib
 
