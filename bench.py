@@ -180,7 +180,20 @@ def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
         "sample": f"{nseg} of {nseg_total} segments ({nseg * seg_len} B), {units} (group, segment) "
                   f"units, {dt:.1f} s" + ("; --unique (.* states)" if uq else ""),
         "stats": st, "sample_bytes": nseg * seg_len, "sample_reports": int(len(reps)),
+        "seconds": dt,
     }
+
+
+def cpu_warmup(groups, data, seg_len, n, nbytes=64 << 10):
+    """n untimed warm-up runs of the oracle on the first nbytes of the stream
+    (one segment, all host threads); returns their description."""
+    from oracle import oracle
+    views = groups.views()
+    uq = has_sticky(views)
+    k = min(nbytes, seg_len, len(data))
+    for _ in range(n):
+        oracle.match(views, data[:k], 1, k, mode=0, unique=uq, nthreads=os.cpu_count() or 1)
+    return f"after {n} untimed warm-up runs on the first {k} B"
 
 
 BATCH_DESC = ("16 NFAs of 2k-200k STEs (literal, Hamming, Levenshtein and dot-star generators), "
@@ -205,7 +218,8 @@ def cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=15.0, cap
                        mode=0, seed=0):
     """The oracle on a bounded sample of batched streams: a seeded random order
     of streams, the first `cap` bytes of each, one stream per host thread,
-    until `seconds` have passed. mode 0 is the reference CPU loop as written,
+    until `seconds` have passed (at least one round). mode 0 is the reference
+    CPU loop as written,
     with --unique for NFAs with `.*` states (see has_sticky); mode 1 gives the
     unique-frontier statistics. Returns MB/s, the sample and frontier stats."""
     from concurrent.futures import ThreadPoolExecutor
@@ -227,7 +241,7 @@ def cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=15.0, cap
     done, nbytes = 0, 0
     stats = {"matched": 0, "matched_deg": 0, "reports_raw": 0, "frontier": 0}
     with ThreadPoolExecutor(ncores) as ex:
-        while done < len(order) and time.time() - t0 < seconds:
+        while done < len(order) and (done == 0 or time.time() - t0 < seconds):
             part = order[done:done + ncores]
             done += len(part)
             for n, st in ex.map(one, part):
@@ -239,7 +253,7 @@ def cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=15.0, cap
     if any(uniq):
         sample += f"; --unique for the {sum(uniq)} NFAs with .* states"
     return {"value": nbytes / dt / 1e6, "unit": "MB/s", "cores": min(ncores, done),
-            "kind": "port", "sample": sample, "bytes": nbytes, "stats": stats}
+            "kind": "port", "sample": sample, "bytes": nbytes, "stats": stats, "seconds": dt}
 
 
 def run_batched(args, warmup, rank, world, local_rank):
@@ -353,8 +367,8 @@ def run_batched(args, warmup, rank, world, local_rank):
                 "kernel": "match_kernel", "kernel_ms": mk}
         if not args.no_cpu_baseline:
             cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of)
-            cb.pop("stats")
-            cb.pop("bytes")
+            for k in ("stats", "bytes", "seconds"):
+                cb.pop(k)
             line["cpu_baseline"] = cb
             fr = cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=8.0, mode=1)
             per = {k: v / max(1, fr["bytes"]) for k, v in fr["stats"].items()}
@@ -465,8 +479,8 @@ def run_serving(args, warmup, rank):
                          "traffic": None}}
     if not args.no_cpu_baseline:
         cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of)
-        cb.pop("stats")
-        cb.pop("bytes")
+        for k in ("stats", "bytes", "seconds"):
+            cb.pop(k)
         line["cpu_baseline"] = cb
     print(json.dumps(line), flush=True)
 
@@ -479,13 +493,17 @@ def run_batched_reference(args, warmup):
     nfas, data, offsets, lengths, nfa_of = W.batched_suite(seed=4)
     groups = [nb.Groups(nb.Nfa.from_string(n["anml"]), group_num=1) for n in nfas]
     per = max(5.0, 60.0 / max(1, args.steps))
-    vals = []
+    for k in range(warmup):  # untimed: one round of streams each
+        cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=0.0, seed=1000 + k)
+    vals, secs = [], []
     for k in range(args.steps):
         cb = cpu_sample_streams(groups, data, offsets, lengths, nfa_of, seconds=per, seed=k)
         vals.append(cb["value"])
+        secs.append(cb["seconds"])
     v = float(np.mean(vals))
+    cb["sample"] += f"; after {warmup} untimed warm-up rounds of one stream per thread"
     line = {"metric": METRIC, "value": v, "unit": "MB/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": warmup, "ms_per_step": None,
+            "steps": args.steps, "warmup": warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": "batched_suite", "desc": BATCH_DESC,
@@ -536,16 +554,17 @@ def main():
         import ngap_b200 as nb
         anml, data, cfg = workload_args(args.workload)
         groups = nb.Groups(nb.Nfa.from_string(anml), group_num=cfg["group_num"])
-        vals = []
-        for _ in range(warmup):
-            pass
+        warm = cpu_warmup(groups, data, cfg["seg_len"], warmup)
+        vals, secs = [], []
         per = max(5.0, 60.0 / max(1, args.steps))
         for _ in range(args.steps):
             cb = cpu_baseline(groups, data, cfg["seg_len"], seconds_hint=per)
             vals.append(cb["value"])
+            secs.append(cb["seconds"])
         v = float(np.mean(vals))
+        cb["sample"] += "; " + warm
         line = {"metric": METRIC, "value": v, "unit": "MB/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": warmup, "ms_per_step": None,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
                 "data": "synthetic (seeded)", "impl": "reference",
                 "config": {"workload": args.workload, "desc": cfg["desc"],
@@ -673,7 +692,7 @@ def main():
                 "kernel": "match_kernel", "kernel_ms": mk}
         if not args.no_cpu_baseline:
             cb = cpu_baseline(groups, data[:n_in], seg_len)
-            for k in ("stats", "sample_bytes", "sample_reports"):
+            for k in ("stats", "sample_bytes", "sample_reports", "seconds"):
                 cb.pop(k)
             line["cpu_baseline"] = cb
         per_byte, sample = frontier_stats(groups, data, seg_len)
