@@ -436,7 +436,7 @@ def run_serving(args, warmup, rank):
         servers[name] = (srv, q)
     # two interleaved rounds of the three schedulers (single runs are noisy)
     lat = {name: [] for name in preds}
-    served, launches, clk_all, dev_ms = {}, 0, None, 0.0
+    served, launches, clk_all, dev_ms, d2h = {}, 0, None, 0.0, 0
     for rnd in range(2):
         for name, (srv, q) in servers.items():
             srv.batches.clear()
@@ -452,6 +452,7 @@ def run_serving(args, warmup, rank):
             if name == "learned" and rnd == 1:
                 clk_all = clk.summary()
                 dev_ms = sum(b[3] for b in srv.batches)
+                d2h = 12 * sum(len(r.reports) for r in rs)  # u64 report + u32 stream id
     total = sum(len(r.data) for r in reqs)
     peak, peak_kind = load_peaks()
     line = {"metric": METRIC + "; serving p50/p99 latency", "value": served["learned"],
@@ -469,7 +470,8 @@ def run_serving(args, warmup, rank):
             "frontier_prediction_rel_err": err,
             "gpu_launches": launches, "clocks": clk_all,
             "e2e": {"value": served["learned"], "unit": "MB/s", "h2d_bytes_per_step":
-                    int(total / max(1, args.steps)), "d2h_bytes_per_step": None},
+                    int(total / max(1, args.steps)),
+                    "d2h_bytes_per_step": int(d2h / max(1, args.steps))},
             "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
                          "kernel": "match_kernel (batched, learned scheduler)",
                          "achieved": total / (dev_ms / 1e3) / 1e9 if dev_ms else None,
