@@ -212,6 +212,23 @@ void print_vector(const std::vector<uint64_t>& v) {
   printf(v.size() > 40 ? "...\n" : "\n");
 }
 
+// --dump-reports: the sorted unique reports as raw little-endian u64; false,
+// with a message on stderr, when the file cannot be written in full.
+bool dump_reports(const std::string& path, const std::vector<uint64_t>& v) {
+  FILE* df = fopen(path.c_str(), "wb");
+  if (!df) {
+    std::cerr << "Error: cannot open " << path << " for writing" << std::endl;
+    return false;
+  }
+  const size_t n = v.empty() ? 0 : fwrite(v.data(), sizeof(uint64_t), v.size(), df);
+  const bool closed = fclose(df) == 0;
+  if (n != v.size() || !closed) {
+    std::cerr << "Error: writing " << path << " failed" << std::endl;
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -340,7 +357,7 @@ int main(int argc, char** argv) {
     std::cout << "ngap elapsed time: " << ms / 1000.0 << " seconds, throughput = " << thr << " MB/s "
               << std::endl;
   std::cout << "Results number: " << raw << std::endl;
-  bool pass = true;
+  bool pass = true, dump_ok = true;
   if (o.validation) {
     const unsigned long long dupnum = o.duplicate_input_stream > 1 ? o.duplicate_input_stream : 1;
     if (o.report_off) {
@@ -378,22 +395,12 @@ int main(int argc, char** argv) {
         print_vector(ref);
         printf("\n");
       }
-      if (!o.dump_reports.empty()) {
-        FILE* df = fopen(o.dump_reports.c_str(), "wb");
-        if (df) {
-          fwrite(res.data(), sizeof(uint64_t), res.size(), df);
-          fclose(df);
-        }
-      }
+      if (!o.dump_reports.empty()) dump_ok = dump_reports(o.dump_reports, res);
     }
   } else if (!o.dump_reports.empty() && !o.report_off) {
     std::vector<uint64_t> res(uniq);
     if (uniq) ngap_results_copy(eng, res.data(), uniq);
-    FILE* df = fopen(o.dump_reports.c_str(), "wb");
-    if (df) {
-      fwrite(res.data(), sizeof(uint64_t), res.size(), df);
-      fclose(df);
-    }
+    dump_ok = dump_reports(o.dump_reports, res);
   }
   if (!blocking) {
     if (pass)
@@ -409,5 +416,5 @@ int main(int argc, char** argv) {
   ngap_groups_destroy(groups);
   ngap_nfa_destroy(nfa);
   printf("FINISHED!\n");
-  return 0;
+  return dump_ok ? 0 : 255;
 }
