@@ -31,7 +31,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, lib
-from .engine import batch_match_async
+from .engine import as_u8, batch_match_async
 
 REGION = 1 << 14          # bytes per feature region
 ENTROPY_WINDOW = 1024     # bytes per entropy window
@@ -73,7 +73,7 @@ def byte_features(data, offsets, reg_stream, reg_start, reg_len, window=ENTROPY_
     if hasattr(data, "data_ptr"):
         ptr, on_dev, nbytes = data.data_ptr(), 1, data.numel()
     else:
-        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        arr = as_u8(data)
         ptr, on_dev, nbytes = arr.ctypes.data, 0, arr.nbytes
     check(lib().ngap_features(ctypes.c_void_p(ptr), nbytes, on_dev, offs.ctypes.data,
                               lens.ctypes.data, n, window, out.ctypes.data,

@@ -15,6 +15,14 @@ from . import _lib
 from ._lib import ALGORITHMS, NgapError, check, lib
 
 
+def as_u8(data):
+    """Host input as a contiguous uint8 array: bytes-like objects (bytes,
+    bytearray, memoryview) by their bytes, arrays and sequences as values."""
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        return np.frombuffer(data, dtype=np.uint8)
+    return np.ascontiguousarray(data, dtype=np.uint8)
+
+
 class Nfa:
     """Parsed ANML (load_nfa_from_anml, code/src/commons/NFALoader.cpp:70)."""
 
@@ -221,12 +229,16 @@ class Engine:
                              int(report_off), result_capacity, window, chunk, first_segment)
         if hasattr(data, "data_ptr"):
             ptr, on_dev = data.data_ptr(), int(getattr(data, "is_cuda", True))
+            nbytes = data.numel() * data.element_size() if hasattr(data, "numel") else None
         else:
-            arr = np.ascontiguousarray(data, dtype=np.uint8)
+            arr = as_u8(data)
             self._keep = arr
-            ptr, on_dev = arr.ctypes.data, 0
+            ptr, on_dev, nbytes = arr.ctypes.data, 0, arr.nbytes
         if num_seg * seg_len > 0 and ptr == 0:
             raise NgapError(1, "empty input")
+        if nbytes is not None and nbytes < num_seg * seg_len:
+            raise NgapError(1, f"input holds {nbytes} bytes, num_seg * seg_len = "
+                               f"{num_seg * seg_len}")
         check(lib().ngap_match(self._h, tables._h, ctypes.c_void_p(ptr), on_dev, ctypes.byref(p),
                                ctypes.c_void_p(stream or 0)))
 
@@ -344,7 +356,7 @@ def batch_match_async(engine, tableset, data, offsets, lengths, nfas,
     if hasattr(data, "data_ptr"):
         ptr, on_dev, nbytes = data.data_ptr(), int(getattr(data, "is_cuda", True)), data.numel()
     else:
-        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        arr = as_u8(data)
         engine._keep = arr
         ptr, on_dev, nbytes = arr.ctypes.data, 0, arr.nbytes
     check(lib().ngap_batch_match(engine._h, tableset._h, ctypes.c_void_p(ptr), nbytes, on_dev, ss,
@@ -372,7 +384,10 @@ def split_by_stream(reports, stream_ids, nstreams):
 
 def cpu_validate(groups, data, num_seg, seg_len, is_dup=False):
     """The library's CPU checker (the CLI's --validation): sorted unique reports."""
-    arr = np.ascontiguousarray(data, dtype=np.uint8)
+    arr = as_u8(data)
+    if arr.nbytes < num_seg * seg_len:
+        raise NgapError(1, f"input holds {arr.nbytes} bytes, num_seg * seg_len = "
+                           f"{num_seg * seg_len}")
     cap = 1 << 16
     while True:
         out = np.zeros(cap, dtype=np.uint64)
@@ -423,6 +438,7 @@ class Ngap:
         self.groups = None
         self.tables = None
         self.streams = []
+        self.original = None
         self.engine = None
 
     def set_ngap_option(self, opt):
@@ -434,17 +450,54 @@ class Ngap:
         self.opt.group_num = self.groups.count
         return self.groups
 
+    def set_nfa_group(self, groups):
+        self.groups = groups
+
+    def set_report_off(self, report_off, output_capacity, quick_validation=-1):
+        """ngap.h set_report_off (main.cu:106-107): count reports only, the
+        result capacity and the expected report count of --quick-validation."""
+        self.opt.report_off = bool(report_off)
+        self.opt.output_capacity = int(output_capacity)
+        self.opt.quick_validation = int(quick_validation)
+
     def add_symbol_stream(self, seg):
-        self.streams.append(np.ascontiguousarray(seg, dtype=np.uint8))
+        self.streams.append(as_u8(seg).copy())
+
+    def slice_input(self, data):
+        """main.cu:48-51: input_len bytes from input_start_pos (to the end when
+        the input is shorter) when both are set (not -1)."""
+        o = self.opt
+        d = as_u8(data)
+        if o.input_start_pos != -1 and o.input_len != -1:
+            st = min(max(o.input_start_pos, 0), len(d))
+            d = d[st:st + max(o.input_len, 0)]
+        return d
 
     def prepare_segments(self, data):
-        """main.cu:81-102: duplicate, then cut into equal segments."""
+        """main.cu:48-51 and 81-102: slice the input, duplicate it, cut it into
+        equal segments (the whole stream when split_chunk_size <= 0) and keep
+        the duplicated stream (prepare_original_input_streams)."""
         o = self.opt
-        ss = np.tile(np.ascontiguousarray(data, dtype=np.uint8), o.duplicate_input_stream)
+        ss = np.tile(self.slice_input(data), o.duplicate_input_stream)
         chunk = o.split_chunk_size if o.split_chunk_size > 0 else len(ss)
-        num_seg = len(ss) // chunk
+        num_seg = len(ss) // chunk if chunk > 0 else 0
         self.streams = [ss[i * chunk:(i + 1) * chunk] for i in range(num_seg)]
+        self.prepare_original_input_streams(ss)
         return num_seg, chunk
+
+    def prepare_original_input_streams(self, ss):
+        self.original = as_u8(ss)
+
+    def automata_validation(self, results):
+        """ngap::automataValidation (ngap.cu:2270-2344): the reports equal the
+        CPU checker's on the same segments (automataGroupsReference,
+        ngap.cu:2171-2268)."""
+        if self.groups is None:
+            self.preprocessing()
+        data = np.concatenate(self.streams) if self.streams else np.zeros(0, np.uint8)
+        seg_len = len(self.streams[0]) if self.streams else 0
+        want = cpu_validate(self.groups, data, len(self.streams), seg_len, self.is_dup())
+        return bool(np.array_equal(np.asarray(results, dtype=np.uint64), want))
 
     def is_dup(self):
         o = self.opt
