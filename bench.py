@@ -353,7 +353,7 @@ def run_batched(args, warmup, rank, world, local_rank):
                 "data": "synthetic (seeded generators, same shapes as the benchmark config)",
                 "config": {"workload": "batched_suite", "desc": BATCH_DESC, "streams": len(offsets),
                            "nfas": len(nfas), "input_bytes": total, "params": best,
-                           "autotune": [[p, round(ms, 3)] for p, ms in tuned],
+                           "autotune": [[p, round(ms, 3) if ms is not None else None] for p, ms in tuned],
                            "l2": "inputs larger than L2 (2 GiB)"},
                 "reports": {"raw": raw, "unique": uniq},
                 "gpu_launches": launches,

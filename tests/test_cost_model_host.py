@@ -1,5 +1,6 @@
 """Host logic of the learned scheduler and the serving loop (no GPU)."""
 import numpy as np
+import pytest
 
 from ngap_b200 import cost_model as cm
 from ngap_b200 import serving as sv
@@ -96,3 +97,39 @@ def test_serving_admission():
     q = list(reqs)
     s = _server(budget=100, max_bytes=1000, held=(80,))  # the first request does not fit: none
     assert s._form(q) == [] and len(q) == 4
+
+
+def test_autotune_search_with_fake_launches():
+    """The search on the host: every grid point on every tile option, queue
+    overflows skipped, the fastest candidate kept."""
+    from ngap_b200 import autotune as at
+    from ngap_b200.engine import NgapError
+    lengths = np.full(40, 1000, dtype=np.int64)
+    offsets = np.arange(40, dtype=np.int64) * 1000
+    data = np.zeros(40000, np.uint8)
+    nfa_of = np.zeros(40, np.int32)
+    built, calls = [], []
+
+    def make(opts):
+        built.append(opts)
+        return ("ts", opts["tile_mode"])
+
+    def run(engine, ts, buf, offs, lens, nf, stream, params):
+        calls.append((ts, dict(params)))
+        assert len(buf) == int(lens.sum()) and len(offs) == len(lens) == len(nf)
+        if params["queue_capacity"] == 1024:
+            raise NgapError(6, "queue")
+        cost = {"shared": 3.0, "global": 1.0}[ts[1]]
+        return cost * params["window"] / 1024 + (0.5 if params["queue_capacity"] else 0.0)
+
+    grid = {"window": [512, 1024], "queue_capacity": [0, 1024, 4096]}
+    best, table = at.autotune(None, None, data, offsets, lengths, nfa_of, grid=grid, frac=0.1,
+                              reps=2, tile_grid=[{"tile_mode": "shared"}, {"tile_mode": "global"}],
+                              run=run, make_tableset=make)
+    assert built == [{"tile_mode": "shared"}, {"tile_mode": "global"}]
+    assert len(table) == 12 and sum(ms is None for _, ms in table) == 4
+    assert best == {"window": 512, "queue_capacity": 0, "tiles": {"tile_mode": "global"}}
+    # reps + 1 launches per candidate that did not overflow, one for those that did
+    assert len(calls) == 8 * 3 + 4
+    with pytest.raises(ValueError):
+        at.autotune(None, None, data, offsets, lengths, nfa_of, tile_grid=[{}], run=run)
