@@ -138,20 +138,9 @@ namespace {
 // The tiles ngap_tables_build would make, planned on the host.
 int plan_tiles(const char* fn, const ngap_groups* g, const ngap_table_opts* opts,
                std::vector<TileHost>& tiles) {
-  ngap_table_opts o{};
-  o.precompute_cutoff = -1;
-  if (opts) o = *opts;
-  if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth ||
-      o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
-    set_error("%s: precompute_depth must be in -1..%d and tile_mode 0..2", fn, kMaxDepth);
-    return NGAP_E_INVALID;
-  }
   TableOpts to;
-  to.precompute_depth = o.precompute_depth;
-  to.precompute_cutoff = o.precompute_cutoff;
-  to.tile_states = o.tile_states;
-  to.max_table_entries = o.max_table_entries;
-  to.tile_mode = o.tile_mode;
+  const int rc = table_opts_from(opts, fn, to, nullptr);
+  if (rc != NGAP_OK) return rc;
   return build_tiles(g->gs, to, tiles);
 }
 

@@ -227,27 +227,14 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     return NGAP_E_INVALID;
   }
   *out = nullptr;
-  ngap_table_opts o{};
-  o.precompute_cutoff = -1;
-  if (opts) o = *opts;
-  if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth) {
-    set_error("precompute_depth must be in -1..%d (got %d)", kMaxDepth, o.precompute_depth);
-    return NGAP_E_INVALID;
-  }
-  if (o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
-    set_error("tile_mode must be NGAP_TILES_AUTO, _SHARED or _GLOBAL (got %d)", o.tile_mode);
-    return NGAP_E_INVALID;
-  }
-  std::unique_ptr<ngap_tables> t(new ngap_tables());
-  t->device = o.device;
-  CUDA_TRY(cudaSetDevice(o.device));
   TableOpts to;
-  to.precompute_depth = o.precompute_depth;
-  to.precompute_cutoff = o.precompute_cutoff;
-  to.tile_states = o.tile_states;
-  to.max_table_entries = o.max_table_entries;
-  to.tile_mode = o.tile_mode;
-  int rc = build_tiles(g->gs, to, t->tiles);
+  int device = 0;
+  int rc = table_opts_from(opts, "ngap_tables_build", to, &device);
+  if (rc != NGAP_OK) return rc;
+  std::unique_ptr<ngap_tables> t(new ngap_tables());
+  t->device = device;
+  CUDA_TRY(cudaSetDevice(device));
+  rc = build_tiles(g->gs, to, t->tiles);
   if (rc != NGAP_OK) return rc;
   t->num_groups = (int)g->gs.groups.size();
   for (auto& th : t->tiles) {

@@ -752,4 +752,26 @@ int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>
   return NGAP_OK;
 }
 
+int table_opts_from(const ngap_table_opts* opts, const char* fn, TableOpts& out, int* device) {
+  ngap_table_opts o{};
+  o.precompute_cutoff = -1;
+  if (opts) o = *opts;
+  if (o.precompute_depth < -1 || o.precompute_depth > kMaxDepth) {
+    set_error("%s: precompute_depth must be in -1..%d (got %d)", fn, kMaxDepth, o.precompute_depth);
+    return NGAP_E_INVALID;
+  }
+  if (o.tile_mode < NGAP_TILES_AUTO || o.tile_mode > NGAP_TILES_GLOBAL) {
+    set_error("%s: tile_mode must be NGAP_TILES_AUTO, _SHARED or _GLOBAL (got %d)", fn, o.tile_mode);
+    return NGAP_E_INVALID;
+  }
+  out = TableOpts();
+  out.precompute_depth = o.precompute_depth;
+  out.precompute_cutoff = o.precompute_cutoff;
+  out.tile_states = o.tile_states;
+  out.max_table_entries = o.max_table_entries;
+  out.tile_mode = o.tile_mode;
+  if (device) *device = o.device;
+  return NGAP_OK;
+}
+
 }  // namespace ngap

@@ -75,4 +75,8 @@ inline int64_t image_bytes(int64_t n, int cw) {
 // Splits every group into tiles and builds each tile's tables.
 int build_tiles(const GroupSet& gs, const TableOpts& opts, std::vector<TileHost>& tiles);
 
+// Checks the public table options (NULL = the defaults) and converts them;
+// `fn` names the entry point in the error message. *device gets the device.
+int table_opts_from(const ngap_table_opts* opts, const char* fn, TableOpts& out, int* device);
+
 }  // namespace ngap
