@@ -15,6 +15,18 @@ from . import _lib
 from ._lib import ALGORITHMS, NgapError, check, lib
 
 
+TILE_MODES = {"auto": 0, "shared": 1, "global": 2}
+
+
+def table_opts(device, precompute_depth, precompute_cutoff, tile_states, max_table_entries,
+               tile_mode):
+    """ngap_table_opts from Python values; tile_mode is one of TILE_MODES."""
+    if tile_mode not in TILE_MODES:
+        raise ValueError(f"tile_mode must be one of {sorted(TILE_MODES)}")
+    return _lib.TableOpts(device, precompute_depth, precompute_cutoff, tile_states,
+                          max_table_entries, TILE_MODES[tile_mode])
+
+
 def as_u8(data):
     """Host input as a contiguous uint8 array: bytes-like objects (bytes,
     bytearray, memoryview) by their bytes, arrays and sequences as values."""
@@ -118,11 +130,7 @@ class Groups:
 
     @staticmethod
     def _plan_opts(precompute_depth, tile_states, tile_mode, max_table_entries):
-        modes = {"auto": 0, "shared": 1, "global": 2}
-        if tile_mode not in modes:
-            raise ValueError(f"tile_mode must be one of {sorted(modes)}")
-        return _lib.TableOpts(0, precompute_depth, -1, tile_states, max_table_entries,
-                              modes[tile_mode])
+        return table_opts(0, precompute_depth, -1, tile_states, max_table_entries, tile_mode)
 
     def tiles(self, precompute_depth=0, tile_states=0, tile_mode="auto", max_table_entries=0):
         """The tiles Tables(...) would build, planned on the host (no GPU):
@@ -180,11 +188,8 @@ class Tables:
 
     def __init__(self, groups, device=0, precompute_depth=0, precompute_cutoff=-1,
                  tile_states=0, max_table_entries=0, tile_mode="auto"):
-        modes = {"auto": 0, "shared": 1, "global": 2}
-        if tile_mode not in modes:
-            raise ValueError(f"tile_mode must be one of {sorted(modes)}")
-        opts = _lib.TableOpts(device, precompute_depth, precompute_cutoff, tile_states,
-                              max_table_entries, modes[tile_mode])
+        opts = table_opts(device, precompute_depth, precompute_cutoff, tile_states,
+                          max_table_entries, tile_mode)
         h = ctypes.c_void_p()
         check(lib().ngap_tables_build(groups._h, ctypes.byref(opts), ctypes.byref(h)))
         self._h = h

@@ -87,6 +87,9 @@ def test_bad_options_are_errors():
     g = _groups(anml, 1)
     with pytest.raises(nb.NgapError):
         g.tiles(precompute_depth=13)
+    for bad in (lambda: g.tiles(tile_mode="tiles"), lambda: nb.Tables(g, tile_mode="tiles")):
+        with pytest.raises(ValueError):  # checked before any device work
+            bad()
     assert g.tiles(precompute_depth=-1)[0]["depth"] >= 1
 
 
