@@ -1,13 +1,15 @@
 """Seeded differential test of the front-end (CPU): random automata and random
-symbol sets through the product's ANML loader and preprocessing and through
-the reference's own front-end sources compiled into oracle/_ref/ref_frontend
+symbol sets through the product's ANML loader and preprocessing, through the
+oracle's pure-Python restatement (oracle/frontend.py) and through the
+reference's own front-end sources compiled into oracle/_ref/ref_frontend
 (NFALoader / NFA / nfa_utils / vasim_helper, code/src/commons). Group graphs
 must be identical, and an input that the reference rejects must be an error
-here too. Skipped where oracle/_ref was not built (it needs the reference
+in both. Skipped where oracle/_ref was not built (it needs the reference
 sources at build time)."""
 import os
 import random
 import subprocess
+import xml.etree.ElementTree as ET
 
 import numpy as np
 import pytest
@@ -46,15 +48,27 @@ def _product(anml, g):
         return None
 
 
-def _assert_same(prod, ref):
+def _python(anml, g):
+    """Group graphs of the oracle's restatement, or None when it rejects the file."""
+    try:
+        nodes, adj = frontend.load_anml(anml)
+        return frontend.build_groups(nodes, adj, g)
+    except (frontend.ParseError, ET.ParseError, ValueError):
+        return None
+
+
+def _assert_same(prod, ref, py):
     if ref is None or len(ref) == 0:  # rejected, or every CC dropped: an error here
         assert prod is None
+        assert py is None or len(py) == 0
         return
     assert prod is not None and prod.count == len(ref)
+    assert py is not None and len(py) == len(ref)
     for gi in range(prod.count):
         v = prod.view(gi)
         for k in KEYS:
             assert np.array_equal(np.asarray(getattr(v, k)), np.asarray(ref[gi][k])), (gi, k)
+            assert np.array_equal(np.asarray(py[gi][k]), np.asarray(ref[gi][k])), (gi, k, "py")
 
 
 @pytest.mark.parametrize("seed", range(40))
@@ -64,7 +78,7 @@ def test_random_degree_automata(built, tmp_path, seed):
     rng = np.random.default_rng(1000 + seed)
     anml = degree_stress(1000 + seed, int(rng.integers(1, 12)), float(rng.random() * 0.6))
     for g in (1, 2, 5):
-        _assert_same(_product(anml, g), _reference(tmp_path, anml, g))
+        _assert_same(_product(anml, g), _reference(tmp_path, anml, g), _python(anml, g))
 
 
 TOKENS = ["a", "z", "-", "^", "[", "]", "\\x41", "\\x7f", "\\xff", "\\n", "\\t", "\\d", "\\w",
@@ -87,6 +101,6 @@ def test_random_symbol_sets(built, tmp_path, seed):
                   symbol_set=("[" + body + "]") if rng.random() < 0.7 else body)
         anml = w.text()
         ref = _reference(tmp_path, anml, 1)
-        _assert_same(_product(anml, 1), ref)
+        _assert_same(_product(anml, 1), ref, _python(anml, 1))
         valid += ref is not None
     assert valid > 0
