@@ -98,3 +98,28 @@ def test_cli_help_and_new_flags():
     assert r.returncode == 0 and "--tile-mode" in r.stdout and "usage: ngap" in r.stdout
     r = subprocess.run([CLI, "--tile-mode", "x"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unable to convert" in r.stderr
+
+
+def test_cli_host_flow_before_the_device():
+    """main.cu:45-102 before any device work: input slicing (shorter input
+    sliced to its end), duplication, segment count, CC statistics. Without a
+    GPU the command stops at the first device call with 255; with one it runs on."""
+    apple = os.path.join(ROOT, "tests", "golden", "apple.anml")
+    inp = os.path.join(ROOT, "tests", "golden", "apple_input.txt")
+    r = subprocess.run([CLI, "-a", apple, "-i", inp, "--algorithm", "nonblockinggroups",
+                        "--group-num=1", "--input-start-pos=70", "--input-len=50",
+                        "--duplicate-input-stream=3", "--split-entire-inputstream-to-chunk-size=4",
+                        "--unique=yes", "--validation=0"], capture_output=True, text=True, timeout=120)
+    out = r.stdout
+    assert r.returncode in (0, 255), r.stdout + r.stderr
+    assert "input_stream_size = 81" in out
+    assert "the input is shorter than the length specified, just slice to end" in out
+    assert "total_state_number = 5" in out and "num_succeed 1, num_fail 0" in out
+    assert "grouped_nfas.size = 1 pl.num_seg=8" in out  # 3 x 11 bytes in 4-byte segments
+    assert "dup_input_stream = 3" in out and "split_entire_inputstream_to_chunk_size = 4" in out
+    r = subprocess.run([CLI, "-a", apple, "-i", inp, "--unique=maybe"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "Unable to convert 'maybe'" in r.stderr
+    r = subprocess.run([CLI, "-a", apple, "-i", os.path.join(ROOT, "no_such_input")],
+                       capture_output=True, text=True)
+    assert r.returncode == 255 and "no such input file" in r.stdout
