@@ -154,7 +154,8 @@ int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_
  * (code/src/ngap/ngap.cu:2358-2468, precompute_table.h:8-101). For key k,
  * ids[off[k] .. off[k+1]) are the report ids (group-local sid | group << 22)
  * of the listed states and reports[roff[k] .. roff[k+1]) those of its report
- * states; off and roff hold nkeys + 1 entries and ids and reports room for
+ * states (in an activation tile, phase 1, a sticky state's id is its
+ * activation slot); off and roff hold nkeys + 1 entries and ids and reports room for
  * cap entries each. When cap is too small the call returns NGAP_E_INVALID
  * with off[nkeys] and roff[nkeys] set to the entries needed. */
 int ngap_tiles_lookup(const ngap_groups* g, const ngap_table_opts* opts, int tile,
