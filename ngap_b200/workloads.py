@@ -8,7 +8,7 @@ text plus the input bytes.
   literal_set       64 literals of 8-16 printable bytes, 10% of positions
                     widened to classes of 2-20 symbols, all-input starts;
                     1 MiB uniform printable input, one planted occurrence per
-                    16 KiB.                                      (~1.2k STEs)
+                    16 KiB.                   (786 STEs; the config estimates ~1.2k)
   hamming_set       1000 random ACGT 25-mers, <= 3 substitutions; 16 MiB of
                     uniform ACGT with mutated copies every 64 KiB. Each 25-mer
                     has a matched and a mismatched STE per (position, errors),
@@ -19,7 +19,8 @@ text plus the input bytes.
                     from a Zipf(1.1) symbol law; a fraction of the .* states is
                     always active.
   high_frontier     500 Levenshtein + 2000 dot-star regexes; 16 MiB ACGT +
-                    16 MiB Zipf ASCII.
+                    16 MiB Zipf ASCII.   (101k STEs: 135 per Levenshtein 20-mer,
+                    17 per dot-star regex; the config estimates ~250k)
 """
 import numpy as np
 
@@ -61,6 +62,9 @@ def _sample_from(rng, cls, n):
 
 def literal_set(seed=1, n_patterns=64, len_lo=8, len_hi=16, class_frac=0.10, class_lo=2,
                 class_hi=20, input_len=1 << 20, plant_every=16 << 10):
+    """Literals with a few widened positions (the plain single-stream shape):
+    (ANML, uniform printable input with occurrences planted every
+    plant_every bytes)."""
     rng = np.random.default_rng(seed)
     w = AnmlWriter("literal_set")
     pats = []
@@ -111,6 +115,8 @@ def _hamming_pattern(w, tag, pat, d):
 
 
 def hamming_set(seed=2, n_patterns=1000, k=25, d=3, input_len=16 << 20, plant_every=64 << 10):
+    """Hamming-distance k-mer automata (<= d substitutions): (ANML, uniform
+    ACGT input with copies carrying 0..d substitutions every plant_every)."""
     rng = np.random.default_rng(seed)
     w = AnmlWriter("hamming_set")
     pats = rng.choice(ACGT, size=(n_patterns, k))
@@ -177,6 +183,9 @@ def _levenshtein_pattern(w, tag, pat, d):
 
 def levenshtein_set(seed=3, n_patterns=500, k=20, d=2, input_len=16 << 20, plant_every=64 << 10,
                     writer=None, rng=None):
+    """Edit-distance (<= d) automata on ACGT k-mers: (ANML, uniform ACGT input
+    with edited copies every plant_every). With `writer` the STEs go into
+    that writer and the ANML returned is None."""
     rng = rng if rng is not None else np.random.default_rng(seed)
     w = writer if writer is not None else AnmlWriter("levenshtein_set")
     pats = rng.choice(ACGT, size=(n_patterns, k))
@@ -199,6 +208,8 @@ def levenshtein_set(seed=3, n_patterns=500, k=20, d=2, input_len=16 << 20, plant
 
 
 def zipf_ascii(rng, n, s=1.1):
+    """(symbol order, probabilities, n bytes) of a Zipf(s) law over printable
+    ASCII in a random symbol order."""
     ranks = np.arange(1, len(PRINTABLE) + 1, dtype=np.float64)
     prob = ranks ** (-s)
     prob /= prob.sum()
@@ -208,6 +219,10 @@ def zipf_ascii(rng, n, s=1.1):
 
 def dotstar_set(seed=4, n_patterns=2000, lit_lo=6, lit_hi=10, aas_frac=0.30, input_len=16 << 20,
                 plant_every=64 << 10, writer=None, rng=None, zipf_s=1.1):
+    """literal .* literal regexes over Zipf ASCII, the .* always active in a
+    fraction aas_frac of them: (ANML, Zipf input with both literals planted
+    every plant_every, up to 15 bytes apart). With `writer` as in
+    levenshtein_set."""
     rng = rng if rng is not None else np.random.default_rng(seed)
     w = writer if writer is not None else AnmlWriter("dotstar_set")
     perm, prob, data = zipf_ascii(rng, input_len, zipf_s)
@@ -237,6 +252,8 @@ def dotstar_set(seed=4, n_patterns=2000, lit_lo=6, lit_hi=10, aas_frac=0.30, inp
 
 
 def high_frontier(seed=3, n_lev=500, n_dot=2000, half=16 << 20):
+    """The high-frontier mix: Levenshtein automata over the first half of the
+    input (ACGT) and dot-star regexes over the second (Zipf ASCII)."""
     rng = np.random.default_rng(seed)
     w = AnmlWriter("high_frontier")
     _, dna = levenshtein_set(n_patterns=n_lev, input_len=half, writer=w, rng=rng)
