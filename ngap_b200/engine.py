@@ -43,12 +43,14 @@ class Nfa:
 
     @classmethod
     def from_file(cls, path):
+        """Loads an ANML file (load_nfa_from_file, NFALoader.cpp:164-171)."""
         h = ctypes.c_void_p()
         check(lib().ngap_nfa_load_anml(str(path).encode(), ctypes.byref(h)))
         return cls(h.value)
 
     @classmethod
     def from_string(cls, xml):
+        """Parses an ANML document held in memory (str or bytes)."""
         data = xml.encode() if isinstance(xml, str) else bytes(xml)
         h = ctypes.c_void_p()
         check(lib().ngap_nfa_parse_anml(data, len(data), ctypes.byref(h)))
@@ -103,14 +105,20 @@ class Groups:
 
     @property
     def count(self):
+        """Number of groups (at most group_num; fewer when there are fewer CCs)."""
         return lib().ngap_groups_count(self._h)
 
     def cc_stats(self):
+        """(CCs, CCs whose out-degree could not be limited, CCs over
+        max_nfa_size), as limit_out_degree_on_ccs counts them
+        (nfa_utils.cpp:637-680)."""
         t, f, b = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         check(lib().ngap_groups_cc_stats(self._h, ctypes.byref(t), ctypes.byref(f), ctypes.byref(b)))
         return t.value, f.value, b.value
 
     def view(self, g):
+        """Group g's graph as numpy views of the library's arrays (CSR, bitsets,
+        attributes, always-active and start lists; graph.cu:169-206)."""
         v = _lib.GroupView()
         check(lib().ngap_group_view_get(self._h, g, ctypes.byref(v)))
         V, E = v.num_states, v.num_edges
@@ -248,6 +256,7 @@ class Engine:
                                ctypes.c_void_p(stream or 0)))
 
     def sync(self):
+        """Waits for the engine's last match; raises NgapError on its status."""
         return check(lib().ngap_engine_sync(self._h))
 
     def set_trace(self, enable=True):
@@ -272,11 +281,13 @@ class Engine:
         return lib().ngap_engine_device_bytes(self._h)
 
     def match(self, tables, data, num_seg, seg_len, **kw):
+        """match_async, sync and results: sorted unique reports (uint64)."""
         self.match_async(tables, data, num_seg, seg_len, **kw)
         self.sync()
         return self.results()
 
     def counts(self):
+        """(raw reports emitted, unique reports) of the last match."""
         raw, uniq = ctypes.c_uint64(), ctypes.c_uint64()
         check(lib().ngap_results_count(self._h, ctypes.byref(raw), ctypes.byref(uniq)))
         return raw.value, uniq.value
@@ -295,14 +306,17 @@ class Engine:
         return lib().ngap_results_device(self._h)
 
     def times_ms(self):
+        """(match ms, sort ms) of the last match, from CUDA events."""
         a, b = ctypes.c_float(), ctypes.c_float()
         check(lib().ngap_last_times_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
     def launches(self):
+        """Kernels the last match launched."""
         return lib().ngap_last_launches(self._h)
 
     def work(self):
+        """(worklist entries expanded, entries injected) of the last match."""
         a, b = ctypes.c_uint64(), ctypes.c_uint64()
         check(lib().ngap_engine_work(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
@@ -450,6 +464,8 @@ class Ngap:
         self.opt = opt
 
     def preprocessing(self):
+        """ngap::preprocessing + group_nfas_by_num (ngap.cu:63-91,
+        nfa_utils.cpp:382-424)."""
         o = self.opt
         self.groups = Groups(self.nfa, o.group_num, o.max_nfa_size, o.quit_degree, o.remove_degree)
         self.opt.group_num = self.groups.count
@@ -505,10 +521,13 @@ class Ngap:
         return bool(np.array_equal(np.asarray(results, dtype=np.uint64), want))
 
     def is_dup(self):
+        """Start-of-data states in every segment (ngap_buffer.cu:479-484)."""
         o = self.opt
         return o.duplicate_input_stream > 1 and (o.split_chunk_size in (-1, o.input_len))
 
     def launch(self, algorithm=None):
+        """Builds tables and an engine once, matches the segments and returns
+        the sorted unique reports (the launch_*_groups bodies, ngap.cu:115-2078)."""
         o = self.opt
         if self.groups is None:
             self.preprocessing()
