@@ -475,7 +475,7 @@ class Ngap:
         self.groups = groups
 
     def set_report_off(self, report_off, output_capacity, quick_validation=-1):
-        """ngap.h set_report_off (main.cu:106-107): count reports only, the
+        """ngap.h set_report_off (main.cu:105-106): count reports only, the
         result capacity and the expected report count of --quick-validation."""
         self.opt.report_off = bool(report_off)
         self.opt.output_capacity = int(output_capacity)
