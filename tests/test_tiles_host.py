@@ -180,3 +180,32 @@ def test_table_lookup_arguments():
     with pytest.raises(ValueError):
         g.table_lookup(0, np.zeros(3, np.uint8))
     assert g.table_lookup(0, np.zeros((0, 1), np.uint8), precompute_depth=2) == []
+
+
+@pytest.mark.parametrize("seed", range(100))
+def test_prefix_tables_random_automata(seed):
+    """Random automata with fan-out hubs, self-loops and dense CCs (no sticky
+    states, so every tile is a plain one): the union over all tiles of one
+    key's lists equals the definition restated on the whole group set, for
+    every tile mode and every depth the tiles have."""
+    from golden.make_golden import degree_stress
+    rng = np.random.default_rng(seed)
+    anml = degree_stress(seed, int(rng.integers(1, 12)), float(rng.random() * 0.5))
+    try:
+        groups = _groups(anml, int(rng.integers(1, 4)))
+    except nb.NgapError:  # every CC dropped by the degree limiter
+        return
+    views = groups.views()
+    for mode in ("shared", "global", "auto"):
+        kw = dict(precompute_depth=int(rng.integers(1, 6)), tile_mode=mode)
+        tiles = groups.tiles(**kw)
+        assert all(t["phase"] == 0 for t in tiles)
+        for d in range(1, min(t["depth"] for t in tiles) + 1):
+            keys = rng.integers(97, 104, size=(40, d)).astype(np.uint8)  # 'g' is never accepted
+            got = [(set(), set()) for _ in keys]
+            for ti in range(len(tiles)):
+                for k, (ids, reps) in enumerate(groups.table_lookup(ti, keys, **kw)):
+                    got[k][0].update(ids.tolist())
+                    got[k][1].update(reps.tolist())
+            want = _expected_lists(views, range(len(views)), keys)
+            assert [(sorted(a), sorted(b)) for a, b in got] == want, (mode, d)
