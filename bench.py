@@ -16,7 +16,14 @@ slowest rank's time.
 
 `--impl reference` times the reference CPU matcher (the oracle's restatement
 of automataGroupsReference, code/src/ngap/ngap.cu:2171-2268) on a bounded
-sample of the same workload with all host threads.
+sample of the same workload with all host threads, after W untimed warm-up
+samples; ms_per_step is the mean sample time.
+
+Other workloads (`--workload`): literal_set (plain single stream; its line
+also compares blockinggroups with nonblockingallgroups), high_frontier,
+batched_suite (4096 streams, 16 NFAs, one launch per step, autotuned) and
+serving (Poisson arrivals; p50/p99 latency per scheduler and the frontier
+prediction error of each predictor).
 """
 import argparse
 import json
