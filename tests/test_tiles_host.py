@@ -209,3 +209,113 @@ def test_prefix_tables_random_automata(seed):
                     got[k][1].update(reps.tolist())
             want = _expected_lists(views, range(len(views)), keys)
             assert [(sorted(a), sorted(b)) for a, b in got] == want, (mode, d)
+
+
+def _random_star_nfa(rng, nccs):
+    """CCs of literal chains with `.*` states (some always active, some
+    reporting), extra forward edges and, now and then, a back edge."""
+    w = W.AnmlWriter("stars")
+    for c in range(nccs):
+        n = int(rng.integers(3, 9))
+        kinds = ["lit"] * n
+        for i in range(1, n - 1):
+            if rng.random() < 0.35:
+                kinds[i] = "aas" if rng.random() < 0.25 else "star"
+        edges = {i: set() for i in range(n)}
+        for i in range(n - 1):
+            edges[i].add(i + 1)
+            if kinds[i] in ("star", "aas"):
+                edges[i].add(i)
+        for _ in range(int(rng.integers(0, 3))):  # extra forward edges
+            a = int(rng.integers(0, n - 1))
+            edges[a].add(int(rng.integers(a + 1, n)))
+        if rng.random() < 0.2:  # a back edge: a cycle through non-sticky states
+            a = int(rng.integers(1, n))
+            edges[a].add(int(rng.integers(0, a)))
+        for i in range(n):
+            nm = f"c{c}v{i}"
+            tg = [f"c{c}v{j}" for j in sorted(edges[i])]
+            if kinds[i] == "lit":
+                w.ste(nm, [int(rng.integers(97, 101))], tg, start="all-input" if i == 0 else None,
+                      report=(i == n - 1) or rng.random() < 0.1)
+            else:
+                w.ste(nm, None, tg, symbol_set="*", start="all-input" if kinds[i] == "aas" else None,
+                      report=rng.random() < 0.3)
+    return w.text()
+
+def _classify(views):
+    """The CC classification restated on the group graphs: bounded when the
+    graph without edges into always-active states is acyclic; layered when it
+    is not, it has sticky states (not always-active, every byte, a self-loop),
+    it becomes acyclic without their self-loops and no sticky state reaches
+    another; cyclic otherwise. Per CC: (kind, sticky states)."""
+    out = []
+    for v in views:
+        ro, co = np.asarray(v.row_offsets), np.asarray(v.col_indices)
+        at = np.asarray(v.node_attrs)
+        bits = np.asarray(v.symbol_sets).reshape(-1, 8)
+        cb = np.asarray(v.cc_begin)
+        for c in range(len(cb) - 1):
+            b, e = int(cb[c]), int(cb[c + 1])
+            nodes = range(b, e)
+            aas = lambda u: bool(at[u] & 1)
+            sticky = {u for u in nodes if not aas(u) and np.all(bits[u] == 0xFFFFFFFF) and u in co[ro[u]:ro[u + 1]]}
+            def acyclic(keep):
+                indeg = {u: 0 for u in nodes}
+                for u in nodes:
+                    for x in co[ro[u]:ro[u + 1]]:
+                        if keep(u, int(x)): indeg[int(x)] += 1
+                q = [u for u in nodes if indeg[u] == 0]
+                seen = 0
+                while q:
+                    u = q.pop()
+                    seen += 1
+                    for x in co[ro[u]:ro[u + 1]]:
+                        if keep(u, int(x)):
+                            indeg[int(x)] -= 1
+                            if indeg[int(x)] == 0: q.append(int(x))
+                return seen == len(nodes)
+            if acyclic(lambda u, x: not aas(x)):
+                out.append(("bounded", len(sticky)))
+                continue
+            keep = lambda u, x: not aas(x) and not (u == x and u in sticky)
+            ok = bool(sticky) and acyclic(keep)
+            if ok:  # no sticky state reachable from another
+                for s in sticky:
+                    stack, seen = [s], {s}
+                    while stack and ok:
+                        u = stack.pop()
+                        for x in co[ro[u]:ro[u + 1]]:
+                            x = int(x)
+                            if keep(u, x) and x not in seen:
+                                if x in sticky:
+                                    ok = False
+                                    break
+                                seen.add(x)
+                                stack.append(x)
+            out.append(("layered" if ok else "cyclic", len(sticky)))
+    return out
+
+
+
+@pytest.mark.parametrize("seed", range(60))
+def test_layered_classification_random(seed):
+    """Tile counts per kind match the restated classification in every tile
+    mode: bounded CCs in plain tiles, cyclic ones in cyclic tiles (with their
+    sticky states), layered ones in activation/layered pairs (one activation
+    slot per sticky state)."""
+    rng = np.random.default_rng(seed)
+    anml = _random_star_nfa(rng, int(rng.integers(1, 10)))
+    groups = _groups(anml, int(rng.integers(1, 4)))
+    cl = _classify(groups.views())
+    want = (sum(k == "bounded" for k, _ in cl), sum(k == "cyclic" for k, _ in cl),
+            sum(k == "layered" for k, _ in cl), sum(s for k, s in cl if k == "layered"),
+            sum(s for k, s in cl if k == "cyclic"))
+    for mode in ("auto", "shared", "global"):
+        tiles = groups.tiles(precompute_depth=2, tile_mode=mode)
+        got = (sum(t["num_ccs"] for t in tiles if t["phase"] == 0 and t["max_path"] >= 0),
+               sum(t["num_ccs"] for t in tiles if t["phase"] == 0 and t["max_path"] < 0),
+               sum(t["num_ccs"] for t in tiles if t["phase"] == 2),
+               sum(t["nact"] for t in tiles if t["phase"] == 1),
+               sum(t["nsticky"] for t in tiles if t["phase"] == 0 and t["max_path"] < 0))
+        assert got == want, mode
