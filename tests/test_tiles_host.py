@@ -319,3 +319,88 @@ def test_layered_classification_random(seed):
                sum(t["nact"] for t in tiles if t["phase"] == 1),
                sum(t["nsticky"] for t in tiles if t["phase"] == 0 and t["max_path"] < 0))
         assert got == want, mode
+
+
+def _layered_lists(views, keys):
+    """Prefix-table lists of the layered pairs restated on the group graphs,
+    per key over all layered CCs: (non-sticky states of the activation
+    tables, sticky states they reach, states of the layered tables, their
+    report states). Activation tables start from the always-active states
+    among the states with a path to a sticky state (through non-sticky
+    states) and stop at sticky states; layered tables start from all
+    always-active states and never enter a sticky state."""
+    out = [[set(), 0, set(), set()] for _ in keys]
+    for gi, v in enumerate(views):
+        ro, co = np.asarray(v.row_offsets), np.asarray(v.col_indices)
+        at = np.asarray(v.node_attrs)
+        bits = np.asarray(v.symbol_sets).reshape(-1, 8)
+        cb = np.asarray(v.cc_begin)
+        kinds = _classify([v])
+
+        def succ(u):
+            return [int(x) for x in co[ro[u]:ro[u + 1]] if not at[int(x)] & 1]
+
+        def acc(s, b):
+            return (int(bits[s, b >> 5]) >> (b & 31)) & 1
+
+        for c in range(len(cb) - 1):
+            if kinds[c][0] != "layered":
+                continue
+            nodes = range(int(cb[c]), int(cb[c + 1]))
+            sticky = {u for u in nodes if not at[u] & 1 and np.all(bits[u] == 0xFFFFFFFF)
+                      and u in co[ro[u]:ro[u + 1]]}
+            pre, grew = set(sticky), True
+            while grew:
+                grew = False
+                for u in nodes:
+                    if u not in pre and any(x in pre for x in succ(u)):
+                        pre.add(u)
+                        grew = True
+            for k, key in enumerate(keys):
+                cur = {u for u in nodes if at[u] & 1 and u in pre and acc(u, int(key[0]))}
+                for b in key[1:]:
+                    cur = {x for u in cur if u not in sticky for x in succ(u)
+                           if x in pre and acc(x, int(b))}
+                out[k][0] |= {u | gi << 22 for u in cur if u not in sticky}
+                out[k][1] += len(cur & sticky)
+                cur = {u for u in nodes if at[u] & 1 and acc(u, int(key[0]))}
+                for b in key[1:]:
+                    cur = {x for u in cur for x in succ(u) if x not in sticky and acc(x, int(b))}
+                out[k][2] |= {u | gi << 22 for u in cur}
+                out[k][3] |= {u | gi << 22 for u in cur if at[u] & 2}
+    return out
+
+
+@pytest.mark.parametrize("seed", range(30))
+def test_layered_pair_tables_random(seed):
+    """The activation and layered tiles' prefix tables on random star-heavy
+    automata equal the restated lists (in activation tiles the sticky states
+    are the only reports and their ids are activation slots, so they are
+    compared by count)."""
+    from collections import Counter
+    rng = np.random.default_rng(seed)
+    groups = _groups(_random_star_nfa(rng, int(rng.integers(1, 10))), int(rng.integers(1, 4)))
+    views = groups.views()
+    for mode in ("shared", "global"):
+        kw = dict(precompute_depth=3, tile_mode=mode)
+        tiles = groups.tiles(**kw)
+        act = [i for i, t in enumerate(tiles) if t["phase"] == 1]
+        lay = [i for i, t in enumerate(tiles) if t["phase"] == 2]
+        if not act:
+            continue
+        for d in range(1, min(tiles[i]["depth"] for i in act + lay) + 1):
+            keys = rng.integers(96, 102, size=(30, d)).astype(np.uint8)  # '`' only stars accept
+            got = [[Counter(), 0, set(), set()] for _ in keys]
+            for i in act:
+                for k, (ids, reps) in enumerate(groups.table_lookup(i, keys, **kw)):
+                    got[k][0].update(ids.tolist())
+                    got[k][0].subtract(reps.tolist())
+                    got[k][1] += len(reps)
+            for i in lay:
+                for k, (ids, reps) in enumerate(groups.table_lookup(i, keys, **kw)):
+                    got[k][2] |= set(ids.tolist())
+                    got[k][3] |= set(reps.tolist())
+            want = _layered_lists(views, keys)
+            for k in range(len(keys)):
+                nonsticky = {x for x, n in got[k][0].items() if n > 0}
+                assert (nonsticky, got[k][1], got[k][2], got[k][3]) == tuple(want[k]), (mode, d, k)
