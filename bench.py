@@ -169,6 +169,28 @@ def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
     views = groups.views()
     uq = has_sticky(views)  # the reference's --unique where the loop as written does not end
     nseg_total = len(data) // seg_len
+    # a probe on the first bytes: when one whole segment would take longer
+    # than seconds_hint, the sample is a prefix of the first segment sized to
+    # about seconds_hint (the per-byte cost of the loop is steady)
+    probe = min(seg_len, 16 << 10)
+    t0 = time.time()
+    reps, st = oracle.match(views, data[:probe], 1, probe, mode=0, unique=uq, nthreads=ncores)
+    dt = dt_probe = max(time.time() - t0, 1e-6)
+    if dt_probe * seg_len / probe > seconds_hint:
+        n = int(min(seg_len, max(probe, probe * seconds_hint / dt_probe)))
+        if n > 2 * probe:  # otherwise the probe is the sample
+            t0 = time.time()
+            reps, st = oracle.match(views, data[:n], 1, n, mode=0, unique=uq, nthreads=ncores)
+            dt = time.time() - t0
+        else:
+            n = probe
+        return {
+            "value": n / dt / 1e6, "unit": "MB/s", "cores": min(ncores, len(views)),
+            "kind": "port",
+            "sample": f"first {n} B of segment 0 of {nseg_total} ({len(views)} (group, segment) "
+                      f"units), {dt:.1f} s" + ("; --unique (.* states)" if uq else ""),
+            "stats": st, "sample_bytes": n, "sample_reports": int(len(reps)), "seconds": dt,
+        }
     nseg = 1
     t0 = time.time()
     reps, st = oracle.match(views, data[:seg_len], 1, seg_len, mode=0, unique=uq, nthreads=ncores)
@@ -191,7 +213,7 @@ def cpu_baseline(groups, data, seg_len, seconds_hint=20.0, impl_line=False):
     }
 
 
-def cpu_warmup(groups, data, seg_len, n, nbytes=64 << 10):
+def cpu_warmup(groups, data, seg_len, n, nbytes=16 << 10):
     """n untimed warm-up runs of the oracle on the first nbytes of the stream
     (one segment, all host threads); returns their description."""
     from oracle import oracle
