@@ -10,6 +10,8 @@
  *   always-active states are appended to the next frontier (ngap.cu:2212-2258,
  *   DEBUG_PL_ADVANCE_CONCAT is defined in code/src/ngap/ngap_buffer.h:19);
  *   the loop stops at the segment end or when the frontier is empty.
+ * With validator_quirk the odd-start rule of the validator's loop condition
+ * (see ngap_oracle.h) is reproduced too.
  */
 #define _GNU_SOURCE
 #include "ngap_oracle.h"
@@ -63,8 +65,11 @@ static inline uint64_t to_key(uint32_t id, uint32_t off) { return ((uint64_t)off
 
 static void run_unit(const oracle_group* g, int gi, const uint8_t* input, int64_t seg,
                      int64_t seg_len, int is_dup, int64_t first_seg, int mode, int unique,
-                     vec64* rep, oracle_stats* st) {
+                     int quirk, vec64* rep, oracle_stats* st) {
   const int64_t lo = seg * seg_len, hi = lo + seg_len;
+  /* the reference validator's first test reads frontiers[iter % 2] with iter
+     the segment's first global position (ngap.cu:2212) */
+  if (quirk && ((first_seg + seg) * seg_len) % 2 != 0) return;
   const uint32_t gbits = (uint32_t)gi << 22;
   vec32 cur = {0}, nxt = {0};
   uint8_t* mark = NULL;
@@ -139,7 +144,8 @@ int64_t oracle_last_needed(void) { return g_last_needed; }
 
 int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* input,
                      int64_t num_seg, int64_t seg_len, int is_dup, int64_t first_seg, int mode,
-                     int unique, int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats) {
+                     int unique, int validator_quirk, int nthreads, uint64_t* out, int64_t cap,
+                     oracle_stats* stats) {
   const int64_t units = (int64_t)ngroups * num_seg;
   vec64* reps = (vec64*)calloc((size_t)(units > 0 ? units : 1), sizeof(vec64));
   oracle_stats* sts = (oracle_stats*)calloc((size_t)(units > 0 ? units : 1), sizeof(oracle_stats));
@@ -148,8 +154,8 @@ int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* inp
   for (int64_t u = 0; u < units; u++) {
     int gi = (int)(u / num_seg);
     int64_t seg = u % num_seg;
-    run_unit(&groups[gi], gi, input, seg, seg_len, is_dup, first_seg, mode, unique, &reps[u],
-             &sts[u]);
+    run_unit(&groups[gi], gi, input, seg, seg_len, is_dup, first_seg, mode, unique,
+             validator_quirk, &reps[u], &sts[u]);
   }
   int64_t total = 0;
   oracle_stats acc = {0, 0, 0, 0};

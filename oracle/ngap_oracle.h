@@ -44,10 +44,20 @@ typedef struct oracle_stats {
  * unique reports, or -1 when more than `cap` would be written (stats and the
  * return of oracle_last_needed() still give the count). first_seg is the
  * global index of the first segment (start-of-data states belong to global
- * segment 0 unless is_dup). */
+ * segment 0 unless is_dup).
+ *
+ * validator_quirk = 1 reproduces the reference CPU validator exactly as it
+ * runs, including its loop condition `while (!frontiers[iter % 2].empty() ...)`
+ * (ngap.cu:2212): iter starts at the segment's first global position and the
+ * initial states go to frontiers[0], so a segment that starts at an odd
+ * position (odd seg_len, odd segment index) tests the empty frontiers[1] and
+ * reports nothing. The reference's GPU matchers report those segments; with
+ * validator_quirk = 0 (the default, the engine's semantics) they are matched
+ * like every other segment. */
 int64_t oracle_match(const oracle_group* groups, int ngroups, const uint8_t* input,
                      int64_t num_seg, int64_t seg_len, int is_dup, int64_t first_seg, int mode,
-                     int unique, int nthreads, uint64_t* out, int64_t cap, oracle_stats* stats);
+                     int unique, int validator_quirk, int nthreads, uint64_t* out, int64_t cap,
+                     oracle_stats* stats);
 
 int64_t oracle_last_needed(void);
 

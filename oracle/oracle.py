@@ -44,8 +44,8 @@ def lib():
         L.oracle_match.restype = ctypes.c_int64
         L.oracle_match.argtypes = [ctypes.POINTER(OracleGroup), ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
-                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
-                                   ctypes.c_int64, ctypes.POINTER(OracleStats)]
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(OracleStats)]
         L.oracle_last_needed.restype = ctypes.c_int64
         _L = L
     return _L
@@ -58,10 +58,12 @@ def _field(g, name):
 
 
 def match(groups, data, num_seg, seg_len, is_dup=False, mode=1, unique=False, nthreads=0,
-          first_segment=0):
+          first_segment=0, validator_quirk=False):
     """Returns (sorted unique reports as uint64 in the reference encoding, stats dict).
     `groups` items expose row_offsets, col_indices, symbol_sets, node_attrs,
-    always_active, start_states (dicts or objects)."""
+    always_active, start_states (dicts or objects). validator_quirk reproduces
+    the reference CPU validator's odd-start rule (ngap_oracle.h): segments
+    that start at an odd position report nothing."""
     keep = []
     arr = (OracleGroup * max(1, len(groups)))()
     for i, g in enumerate(groups):
@@ -80,8 +82,8 @@ def match(groups, data, num_seg, seg_len, is_dup=False, mode=1, unique=False, nt
     while True:
         out = np.zeros(cap, dtype=np.uint64)
         n = lib().oracle_match(arr, len(groups), d.ctypes.data, num_seg, seg_len, int(is_dup),
-                               first_segment, mode, int(unique), nthreads, out.ctypes.data, cap,
-                               ctypes.byref(stats))
+                               first_segment, mode, int(unique), int(bool(validator_quirk)),
+                               nthreads, out.ctypes.data, cap, ctypes.byref(stats))
         if n >= 0:
             break
         cap = max(cap * 2, int(lib().oracle_last_needed()) + 1)

@@ -2,29 +2,40 @@
 
 The reference writes no report file, but with --validation it prints the
 sorted unique reports of its GPU run ("Result(N):") and of its CPU validator
-("Reference result(N):", code/src/ngap/ngap.cu:2270-2344) in full when there
-are at most 40. The cases below are small enough for that. For each case and
-algorithm this writes tests/golden/ref_reports/<case>.<algorithm>.json with the
-command's options, both report lists, the raw count and the validation
-verdict, and the case's ANML and input next to them.
+("Reference result(N):", code/src/ngap/ngap.cu:2270-2344): in full when there
+are at most 40, else the first 40.
+
+Two sets of fixtures:
+
+* small cases (at most 40 reports, so both lists are complete) x the seven
+  algorithms: <case>.<algorithm>.json with the command's options, both report
+  lists, the raw count and the validation verdict, and the case's ANML and
+  input next to them;
+* benchmark cases at the benchmark's own sizes (the literal set, 1 MiB, one
+  segment; the first 3 MiB of the Hamming set as 3 x 1 MiB segments, with 1
+  and 10 groups): bench.<case>.<algorithm>.json with the unique count, the
+  first 40 sorted reports of both runs, the verdict and the two elapsed-time
+  lines. Their inputs are regenerated from the seeded generators named in the
+  record, so only the record is committed.
 
 Build the reference first (outputs only in oracle/_ref/):
     make -C oracle -j8 ref-ngap
 then, on a machine with a GPU, from the repo root:
-    python tests/golden/make_ref_reports.py
+    python tests/golden/make_ref_reports.py [--out DIR] [--only small|bench|all]
 """
+import argparse
 import json
 import os
-import re
-import subprocess
 import sys
+import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 from ngap_b200 import workloads as W  # noqa: E402
+from oracle import refcli  # noqa: E402
+from oracle.refcli import parse  # noqa: E402,F401
 
 OUT = os.path.join(ROOT, "tests", "golden", "ref_reports")
-REF = os.path.join(ROOT, "oracle", "_ref", "ngap")
 ALGOS = ["blockinggroups", "NAPgroups", "nonblockinggroups", "nonblockingr1groups",
          "nonblockingr2groups", "nonblockingpcgroups", "nonblockingallgroups"]
 
@@ -49,49 +60,89 @@ def cases():
     yield "dotstar_g2", a, d.tobytes(), dict(group_num=2, split=512, unique=True)
 
 
-def parse(out):
-    def hexes(label):
-        m = re.search(re.escape(label) + r"\((\d+)\):\s*\n([^\n]*)", out)
-        if not m:
-            return None, None
-        vals = [int(x, 16) for x in re.findall(r"0x[0-9a-f]+", m.group(2))]
-        return int(m.group(1)), vals
-    raw = re.search(r"Results number: (\d+)", out)
-    n_gpu, gpu = hexes("Result")
-    n_cpu, cpu = hexes("Reference result")
-    return {"raw": int(raw.group(1)) if raw else None, "unique": n_gpu, "gpu": gpu,
-            "cpu_unique": n_cpu, "cpu": cpu, "validation": "Validation PASS!" in out}
+# benchmark-size cases: (name, generator, seed, input bytes used, options, algorithms)
+BENCH = [
+    ("literal_c1", "literal_set", 1, 1 << 20, dict(group_num=1, split=1 << 20),
+     ["blockinggroups", "nonblockingallgroups"]),
+    ("hamming_c2_g1", "hamming_set", 2, 3 << 20, dict(group_num=1, split=1 << 20),
+     ["nonblockingallgroups"]),
+    ("hamming_c2_g10", "hamming_set", 2, 3 << 20, dict(group_num=10, split=1 << 20),
+     ["nonblockingallgroups"]),
+]
 
 
-def main():
-    if not os.path.exists(REF):
-        raise SystemExit("build the reference first: make -C oracle -j8 ref-ngap")
-    os.makedirs(OUT, exist_ok=True)
+def bench_input(gen, seed, n):
+    """The ANML and the first n input bytes of a benchmark workload."""
+    anml, data = getattr(W, gen)(seed=seed)
+    return anml, data[:n].tobytes()
+
+
+def command(a_path, i_path, n, algo, o, depth):
+    return refcli.command(a_path, i_path, n, algo, o["group_num"], o["split"], depth=depth,
+                          dup=o.get("dup", 1), unique=bool(o.get("unique")))
+
+
+def rel(args):
+    return " ".join(os.path.relpath(x, ROOT) if x.startswith(ROOT) else x for x in args)
+
+
+def small(out):
     for name, anml, data, o in cases():
-        a_path = os.path.join(OUT, name + ".anml")
-        i_path = os.path.join(OUT, name + ".input")
+        a_path = os.path.join(out, name + ".anml")
+        i_path = os.path.join(out, name + ".input")
         open(a_path, "w").write(anml)
         open(i_path, "wb").write(data)
         dup = o.get("dup", 1)
         for algo in ALGOS:
-            args = [REF, "-a", a_path, "-i", i_path, f"--algorithm={algo}",
-                    f"--group-num={o['group_num']}", "--input-start-pos=0",
-                    f"--input-len={len(data)}",
-                    f"--split-entire-inputstream-to-chunk-size={o['split']}",
-                    f"--duplicate-input-stream={dup}", "--validation=true",
-                    "--precompute-depth=2", f"--unique={'true' if o.get('unique') else 'false'}"]
-            r = subprocess.run(args, capture_output=True, text=True, timeout=120)
-            rec = parse(r.stdout)
-            rec.update({"case": name, "algorithm": algo, "returncode": r.returncode,
+            args = command(a_path, i_path, len(data), algo, o, 2)
+            rc, text = refcli.run(args, 120)
+            rec = parse(text)
+            rec.update({"case": name, "algorithm": algo, "returncode": rc,
                         "options": dict(o, dup=dup, input_len=len(data), precompute_depth=2),
-                        "command": " ".join(os.path.relpath(x, ROOT) if x.startswith(ROOT) else x
-                                            for x in args)})
+                        "command": rel(args)})
             complete = rec["unique"] is not None and rec["unique"] <= 40 and rec["gpu"] is not None
             rec["complete"] = bool(complete and len(rec["gpu"]) == rec["unique"])
-            with open(os.path.join(OUT, f"{name}.{algo}.json"), "w") as f:
+            with open(os.path.join(out, f"{name}.{algo}.json"), "w") as f:
                 json.dump(rec, f, indent=1)
-            print(name, algo, "rc", r.returncode, "unique", rec["unique"], "validation",
-                  rec["validation"], "complete", rec["complete"])
+            print(name, algo, "rc", rc, "unique", rec["unique"], "validation",
+                  rec["validation"], "complete", rec["complete"], flush=True)
+
+
+def bench(out, depth=3):
+    tmp = tempfile.mkdtemp(prefix="ngap_ref_")
+    for name, gen, seed, n, o, algos in BENCH:
+        anml, data = bench_input(gen, seed, n)
+        a_path = os.path.join(tmp, name + ".anml")
+        i_path = os.path.join(tmp, name + ".input")
+        open(a_path, "w").write(anml)
+        open(i_path, "wb").write(data)
+        for algo in algos:
+            args = command(a_path, i_path, n, algo, o, depth)
+            rc, text = refcli.run(args, 1500)
+            rec = parse(text)
+            rec.update({"case": name, "algorithm": algo, "returncode": rc,
+                        "workload": {"generator": gen, "seed": seed, "input_bytes": n},
+                        "options": dict(o, dup=1, input_len=n, precompute_depth=depth),
+                        "command": rel(args).replace(tmp, "<tmp>")})
+            with open(os.path.join(out, f"bench.{name}.{algo}.json"), "w") as f:
+                json.dump(rec, f, indent=1)
+            print(name, algo, "rc", rc, "unique", rec["unique"], "cpu_unique",
+                  rec["cpu_unique"], "validation", rec["validation"], "gpu MB/s",
+                  rec["gpu_mbps"], "cpu MB/s", rec["cpu_mbps"], flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=OUT)
+    ap.add_argument("--only", default="all", choices=["small", "bench", "all"])
+    a = ap.parse_args()
+    if not refcli.available():
+        raise SystemExit("build the reference first: make -C oracle -j8 ref-ngap")
+    os.makedirs(a.out, exist_ok=True)
+    if a.only in ("small", "all"):
+        small(a.out)
+    if a.only in ("bench", "all"):
+        bench(a.out)
 
 
 if __name__ == "__main__":
