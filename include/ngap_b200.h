@@ -211,6 +211,26 @@ int ngap_last_launches(const ngap_engine* e);
 int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injected);
 /* Bytes of device memory the engine holds (input copy, reports, per-warp scratch). */
 int64_t ngap_engine_device_bytes(const ngap_engine* e);
+/* The same, by part. The reference allocates its buffers once per run
+ * (NonBlockingBuffer::init_nfagroups, code/src/ngap/ngap_buffer.cu:475-748);
+ * an engine's buffers only grow, so a caller sharing the device (the serving
+ * loop's memory budget) can tell what a larger batch would add. */
+typedef struct ngap_engine_mem {
+  int64_t input;    /* the engine's copy of the input (largest batch so far, padded) */
+  int64_t reports;  /* raw and unique report buffers, sort scratch, stream ids */
+  int64_t scratch;  /* per-warp worklist scratch: overflow stacks, carry lists, bitmaps */
+  int64_t plan;     /* units, tasks, activation slots, unit traces */
+} ngap_engine_mem;
+int ngap_engine_memory(const ngap_engine* e, ngap_engine_mem* out);
+
+/* Test hook for the kernel's one device wait, the mbarrier of a window's
+ * input copy (the reference has no bounded waits; its kernels poll their
+ * worklists, kernel_ngap_OA.cu:142). For the next ngap_match only, unit
+ * `unit` (in plan order) does not issue its first window's copy and every wait
+ * gives up after `wait_rounds` try_wait rounds: that unit's wait runs out with
+ * nothing in flight, and ngap_engine_sync returns NGAP_E_TIMEOUT. The engine
+ * stays usable; the following match runs normally. */
+int ngap_engine_test_wait_timeout(ngap_engine* e, int32_t unit, int32_t wait_rounds);
 
 /* ---- worklist traces ---- */
 
@@ -317,6 +337,13 @@ void ngap_mlp_destroy(ngap_mlp* m);
  * last epoch's mean squared error. FP32 throughout. */
 int ngap_mlp_train(ngap_mlp* m, const float* x, const float* y, int64_t n, int epochs, int batch,
                    float lr, float* loss);
+/* Gradient of the mean squared error over all n samples x[n][in_dim], y[n]
+ * (host arrays) at the current parameters, in the layout of
+ * ngap_mlp_get_params, into grad (host, room for every parameter); *loss
+ * receives the mean squared error. Parameters are not changed: this is the
+ * step ngap_mlp_train feeds to Adam, exposed for checking. */
+int ngap_mlp_gradient(ngap_mlp* m, const float* x, const float* y, int64_t n, float* grad,
+                      float* loss);
 /* y[n] = model(x[n][in_dim]) (host arrays). bf16 = 1 rounds inputs, weights and
  * activations to bfloat16 (FP32 accumulation); 0 computes in FP32. Runs on
  * the model's own stream; allocates only when n exceeds every earlier call. */
@@ -340,13 +367,15 @@ int ngap_reports_sort_unique(ngap_engine* e, const uint64_t* d_in, uint64_t n, u
  * a latency-critical loop where cudaMalloc's implicit synchronisation is not
  * acceptable. The caller passes device input (n reference-encoded reports)
  * and device output (room for n); n must not exceed 262,144 (larger n returns
- * NGAP_E_INVALID). Scratch (about 2 MiB) is a static device array that every
- * GPU loading this library keeps until exit. The first call on a device looks
- * up that array's device address (cudaGetSymbolAddress) with the device
- * current, so make the first call before any stream capture. All calls share
- * the scratch and it keeps the last call's contents; calls that overlap on
- * the GPU race on it. Uses the calling thread's current device; waits for
- * `stream` before returning the unique count in *n_out. */
+ * NGAP_E_INVALID). d_out may be d_in. Scratch (about 2 MiB) is a static
+ * device array that every GPU loading this library keeps until exit. The
+ * first call on a device (and the first after the device's context changes,
+ * e.g. after cudaDeviceReset) looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current. All calls share the
+ * scratch and it keeps the last call's contents; calls that overlap on the
+ * GPU race on it. Uses the calling thread's current device. The call waits
+ * for `stream` before returning the unique count in *n_out, so it must not be
+ * called while `stream` is being captured (it then returns NGAP_E_INVALID). */
 int ngap_reports_sort_unique_noalloc(const uint64_t* d_in, uint64_t n, uint64_t* d_out,
                                      uint64_t* n_out, void* stream);
 

@@ -8,7 +8,9 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libngap_b200.so")
+# NGAP_B200_LIB names another build of the same library (A/B measurements of
+# kernel variants); by default the in-tree build is loaded
+LIB_PATH = os.environ.get("NGAP_B200_LIB") or os.path.join(_HERE, "libngap_b200.so")
 
 NGAP_OK = 0
 STATUS_NAMES = {
@@ -81,6 +83,11 @@ class BatchParams(ctypes.Structure):
                 ("queue_capacity", ctypes.c_int)]
 
 
+class EngineMem(ctypes.Structure):
+    _fields_ = [("input", ctypes.c_int64), ("reports", ctypes.c_int64),
+                ("scratch", ctypes.c_int64), ("plan", ctypes.c_int64)]
+
+
 class UnitTrace(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_int32), ("tile", ctypes.c_int32), ("lo", ctypes.c_int64),
                 ("hi", ctypes.c_int64), ("work", ctypes.c_uint64)]
@@ -139,7 +146,10 @@ SIGNATURES = {
     "ngap_engine_work": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                         ctypes.POINTER(ctypes.c_uint64)]),
     "ngap_engine_device_bytes": (ctypes.c_int64, [ctypes.c_void_p]),
+    "ngap_engine_memory": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(EngineMem)]),
     "ngap_engine_set_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ngap_engine_test_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32,
+                                                     ctypes.c_int32]),
     "ngap_trace_copy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(UnitTrace), ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int64)]),
     "ngap_tables_stats_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TablesStats)]),
@@ -152,6 +162,9 @@ SIGNATURES = {
     "ngap_mlp_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                       ctypes.POINTER(ctypes.c_float)]),
+    "ngap_mlp_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int64, ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_float)]),
     "ngap_mlp_predict": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                         ctypes.c_int, ctypes.c_void_p]),
     "ngap_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,

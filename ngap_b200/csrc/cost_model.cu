@@ -478,6 +478,50 @@ int ngap_mlp_train(ngap_mlp* m, const float* x, const float* y, int64_t n, int e
   return NGAP_OK;
 }
 
+int ngap_mlp_gradient(ngap_mlp* m, const float* x, const float* y, int64_t n, float* grad,
+                      float* loss) {
+  if (!m || !x || !y || !grad || n < 1 || n > (int64_t)1 << 30) {
+    ngap::set_error("ngap_mlp_gradient: bad argument");
+    return NGAP_E_INVALID;
+  }
+  CM_TRY(cudaSetDevice(m->device));
+  float *dx = nullptr, *dy = nullptr;
+  int* didx = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(dx);
+    cudaFree(dy);
+    cudaFree(didx);
+  };
+  std::vector<int> idx(n);
+  for (int64_t i = 0; i < n; i++) idx[i] = (int)i;
+  cudaError_t ce = cudaMalloc(&dx, (size_t)n * m->D * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&dy, (size_t)n * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&didx, (size_t)n * sizeof(int));
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(dx, x, (size_t)n * m->D * sizeof(float), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(dy, y, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(didx, idx.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemset(m->loss, 0, sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMemset(m->G, 0, m->L.total * sizeof(float));
+  if (ce == cudaSuccess) {
+    mlp_grad_kernel<<<(unsigned)((n + kRows - 1) / kRows), kMlpThreads, grad_smem(m->D)>>>(
+        m->P, m->D, dx, dy, didx, (int)n, 1.f / (float)n, m->G, m->loss);
+    ce = cudaGetLastError();
+  }
+  float l = 0.f;
+  if (ce == cudaSuccess) ce = cudaMemcpy(grad, m->G, m->L.total * sizeof(float), cudaMemcpyDeviceToHost);
+  if (ce == cudaSuccess) ce = cudaMemcpy(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost);
+  if (ce == cudaSuccess) ce = cudaMemset(m->G, 0, m->L.total * sizeof(float));
+  cleanup();
+  if (ce != cudaSuccess) {
+    ngap::set_error("ngap_mlp_gradient: %s", cudaGetErrorString(ce));
+    return NGAP_E_CUDA;
+  }
+  if (loss) *loss = l / (float)n;
+  return NGAP_OK;
+}
+
 int ngap_mlp_predict(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y) {
   if (!m || !x || !y || n < 0) {
     ngap::set_error("ngap_mlp_predict: bad argument");

@@ -50,7 +50,9 @@ __host__ __device__ inline uint32_t prefix_hash(uint32_t key) {
 //   [succ][cmask: nstates x cw x u32][rep: ceil(nstates/32) x u32][cls: 256 B]
 // succ: up to 4 tile-local successors per state; narrow tiles (< 32767
 // states) store 4 x u16 (bit 15 = report successor, 0xffff = none), wide
-// ones 4 x u32 (bit 31 = report successor, kNoSucc = none). cmask: bit c of
+// ones 4 x u32 (bit 31 = report successor, kNoSucc = none); fused wide tiles
+// (one class word) follow each state's 4 x u32 with its successors' class
+// masks (4 x u32, 0 for none), a 32-byte record. cmask: bit c of
 // word c/32 = the state accepts byte class c. cls: byte -> class id, live
 // classes first (identity when cw == 8).
 struct TileDev {
@@ -64,6 +66,7 @@ struct TileDev {
   int32_t cw = 8;           // class words per state: 1, 2 or 8
   int32_t nlive = 0;        // live classes: key base; class id nlive = dead
   int32_t narrow = 1;       // 16-bit successors
+  int32_t fused = 0;        // wide, one class word: records of 2 x uint4 (successors, their masks)
   int32_t image_bytes = 0;  // multiple of 16
   int32_t off_cmask = 0, off_rep = 0, off_cls = 0;
   int32_t inj_batch = 32;   // positions injected per worklist refill (prefix tables)

@@ -184,6 +184,10 @@ struct ngap_engine {
   cudaStream_t sort_cs = nullptr;     // capture stream of those graphs
   bool sort_graph_off = false;
   int sort_chain_pending = 0;         // pipeline kernels of the last graph sort, if it ran
+  // test hook for the bounded device wait (ngap_engine_test_wait_timeout): armed for the
+  // next ngap_match only
+  int32_t test_skip_unit = -1;
+  int32_t test_wait_rounds = 0;
 
   ~ngap_engine() {
     cudaFree(d_input);
@@ -255,6 +259,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
     d.cw = th.cw;
     d.nlive = th.nlive;
     d.narrow = th.narrow ? 1 : 0;
+    d.fused = th.fused ? 1 : 0;
     d.image_bytes = (int32_t)th.image.size();
     d.off_cmask = th.off_cmask;
     d.off_rep = th.off_rep;
@@ -1048,6 +1053,10 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
+  mp.wait_rounds = e->test_wait_rounds > 0 ? e->test_wait_rounds : kWaitRounds;
+  mp.skip_copy_unit = e->test_skip_unit;
+  e->test_wait_rounds = 0;  // the hook covers one match
+  e->test_skip_unit = -1;
   if ((rc = trace_buffer(e, st, &mp.unit_work)) != NGAP_OK) return rc;
   e->trace_seg_len = p->seg_len;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
@@ -1142,14 +1151,35 @@ int ngap_engine_work(const ngap_engine* e, uint64_t* expanded, uint64_t* injecte
   return NGAP_OK;
 }
 
+int ngap_engine_memory(const ngap_engine* e, ngap_engine_mem* out) {
+  if (!e || !out) {
+    set_error("ngap_engine_memory: null argument");
+    return NGAP_E_INVALID;
+  }
+  out->input = (int64_t)e->input_cap;
+  out->reports = 3 * 8 * (int64_t)e->rep_cap + 4 * (int64_t)e->hist_cap + 4 * (int64_t)e->stream_ids_cap;
+  out->scratch =
+      (int64_t)e->slots * 4 * ((int64_t)e->carry_cap + e->mark_words + e->ovf_cap + 2 * e->stk_cap);
+  out->plan = 8 * (int64_t)e->act_cap + 16 * (int64_t)e->rows_cap + 8 * (int64_t)e->unit_work_cap +
+              (int64_t)sizeof(UnitDev) * (int64_t)e->units_cap +
+              (int64_t)sizeof(TaskDev) * (int64_t)e->tasks_cap;
+  return NGAP_OK;
+}
+
 int64_t ngap_engine_device_bytes(const ngap_engine* e) {
-  if (!e) return 0;
-  int64_t b = (int64_t)e->input_cap + 3 * 8 * (int64_t)e->rep_cap + 4 * (int64_t)e->hist_cap;
-  b += (int64_t)e->slots * 4 * ((int64_t)e->carry_cap + e->mark_words + e->ovf_cap + 2 * e->stk_cap);
-  b += 8 * (int64_t)e->act_cap + 16 * (int64_t)e->rows_cap + 8 * (int64_t)e->unit_work_cap;
-  b += (int64_t)sizeof(UnitDev) * (int64_t)e->units_cap + (int64_t)sizeof(TaskDev) * (int64_t)e->tasks_cap;
-  b += 4 * (int64_t)e->stream_ids_cap;
-  return b;
+  ngap_engine_mem m;
+  if (ngap_engine_memory(e, &m) != NGAP_OK) return 0;
+  return m.input + m.reports + m.scratch + m.plan;
+}
+
+int ngap_engine_test_wait_timeout(ngap_engine* e, int32_t unit, int32_t wait_rounds) {
+  if (!e || unit < 0 || wait_rounds < 1) {
+    set_error("ngap_engine_test_wait_timeout: needs an engine, a unit >= 0 and wait_rounds >= 1");
+    return NGAP_E_INVALID;
+  }
+  e->test_skip_unit = unit;
+  e->test_wait_rounds = wait_rounds;
+  return NGAP_OK;
 }
 
 int ngap_engine_set_trace(ngap_engine* e, int enable) {
@@ -1472,6 +1502,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
   mp.unit_work = nullptr;
+  mp.wait_rounds = kWaitRounds;
+  mp.skip_copy_unit = -1;
   e->trace_seg_len = 0;
 
   auto enqueue = [&](cudaStream_t qs) -> int {
@@ -1623,10 +1655,32 @@ static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
 std::mutex g_noalloc_mu;
 constexpr int kNoAllocMaxDevices = 64;
 uint8_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+void* g_noalloc_ctx[kNoAllocMaxDevices] = {};  // context the address belongs to
+
+// The calling thread's current CUDA context (driver cuCtxGetCurrent, reached
+// through the runtime's entry-point lookup so that the library does not link
+// the driver library), or nullptr when it cannot be read.
+void* current_context() {
+  using Fn = int (*)(void**);
+  static Fn fn = []() -> Fn {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<Fn>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 // Device address of the scratch array on the current device. In host code
 // g_noalloc_scratch names a host-side stand-in, not device memory, so the
-// address is looked up once per device with that device current.
+// address is looked up with that device current: once per device, and again
+// whenever the device's current context is another one than at the lookup
+// (after cudaDeviceReset, or a context the caller made current), whose
+// address the old one is not.
 int noalloc_scratch(int dev, uint8_t** out) {
   if (dev < 0 || dev >= kNoAllocMaxDevices) {
     set_error("device %d is beyond the %d devices the allocation-free path supports", dev,
@@ -1634,14 +1688,18 @@ int noalloc_scratch(int dev, uint8_t** out) {
     return NGAP_E_INVALID;
   }
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  void* ctx = current_context();
+  if (!g_noalloc_addr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (ce != cudaSuccess) {
+      g_noalloc_addr[dev] = nullptr;
       set_error("cudaGetSymbolAddress of the sort scratch failed: %s", cudaGetErrorString(ce));
       return NGAP_E_CUDA;
     }
     g_noalloc_addr[dev] = static_cast<uint8_t*>(p);
+    // the runtime may have made the primary context current just now
+    g_noalloc_ctx[dev] = ctx ? ctx : current_context();
   }
   *out = g_noalloc_addr[dev];
   return NGAP_OK;
@@ -1679,6 +1737,14 @@ extern "C" int ngap_reports_sort_unique_noalloc(const uint64_t* d_in, uint64_t n
   }
   *n_out = 0;
   if (n == 0) return NGAP_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {  // the call waits for the stream below
+    set_error("ngap_reports_sort_unique_noalloc waits for its stream to return the unique "
+              "count, so it cannot run while that stream is being captured");
+    return NGAP_E_INVALID;
+  }
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   uint8_t* base = nullptr;
@@ -1690,7 +1756,6 @@ extern "C" int ngap_reports_sort_unique_noalloc(const uint64_t* d_in, uint64_t n
       reinterpret_cast<unsigned long long*>(base + kNoAllocKeyBytes + kNoAllocHistBytes);
   int sms = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
   const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(tiles, (uint32_t)sms * 8));
   // 8 digit passes over the offset half and 8 over the id half; an even count

@@ -83,7 +83,12 @@ struct MatchParams {
   uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
   int32_t stk_g_cap;        // kStickyCap
   unsigned long long* unit_work;  // [units]: entries expanded + injected per unit (tracing), or null
+  int32_t wait_rounds;      // try_wait rounds before an mbarrier wait gives up
+  int32_t skip_copy_unit;   // test hook: this unit's first window copy is not issued (-1: none),
+                            // so its wait runs out and the launch reports kErrTimeout
 };
+
+constexpr int32_t kWaitRounds = 1 << 24;  // default bound of an mbarrier wait
 
 constexpr uint32_t kNoAct = 0xffffffffu;
 
@@ -144,19 +149,30 @@ struct TileView {
   const PrefixTableDev* pt;  // the tile's prefix tables (shared-memory copy)
   int cw;
   int narrow;
+  int fused;       // records of 2 x uint4: successors, then their class masks
   uint32_t nlive;  // live classes: base of the prefix-table keys
   uint32_t rep_levels;  // bit d: the depth-(d+1) table has report lists
 };
 
 // Successors of v in the 32-bit convention (bit 31 = report, kNoSucc = none).
 __device__ __forceinline__ uint4 load_succ(const TileView& tv, uint32_t v) {
-  if (!tv.narrow) return tv.succ[v];
+  if (!tv.narrow) return tv.succ[(size_t)v << tv.fused];
   const uint2 x = tv.succ2[v];
   auto wide = [](uint32_t h) {
     return h == 0xffffu ? kNoSucc : ((h & 0x7fffu) | ((h & 0x8000u) << 16));
   };
   return make_uint4(wide(x.x & 0xffffu), wide(x.x >> 16), wide(x.y & 0xffffu), wide(x.y >> 16));
 }
+
+// Fused tiles: the class masks of v's four successors (0 where none), the
+// second half of v's 32-byte record.
+__device__ __forceinline__ uint4 load_smask(const TileView& tv, uint32_t v) {
+  return tv.succ[((size_t)v << 1) + 1];
+}
+
+// Successor j of a state accepts class c: from the record's masks (fused
+// tiles) or from the successor's own class mask.
+__device__ __forceinline__ bool succ_accepts(const TileView& tv, uint32_t u, uint32_t m, uint32_t c);
 
 // Everything about the current unit and window.
 struct UnitCtx {
@@ -191,9 +207,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// Bounded wait for the mbarrier phase with the given parity; false = gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 24); it++) {
+// Bounded wait for the mbarrier phase with the given parity: at most `rounds`
+// try_wait rounds; false = gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t rounds) {
+  for (int32_t it = 0; it < rounds; it++) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -207,6 +224,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 __device__ __forceinline__ bool accepts(const TileView& tv, uint32_t v, uint32_t c) {
   return (tv.cmask[(size_t)v * tv.cw + (c >> 5)] >> (c & 31)) & 1u;
+}
+
+__device__ __forceinline__ bool succ_accepts(const TileView& tv, uint32_t u, uint32_t m, uint32_t c) {
+  if (tv.fused) return (m >> c) & 1u;  // m = 0 when there is no successor
+  return u != kNoSucc && accepts(tv, u & kIdMask, c);
 }
 
 __device__ __forceinline__ bool is_report(const TileView& tv, uint32_t v) {
@@ -588,6 +610,130 @@ __device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem&
                                                  const TileView& tv, const UnitCtx& c, int lane,
                                                  int r0, int batch);
 
+// Always-active states through the prefix tables for window offsets
+// [r0, r0 + batch), batch <= 64, two positions per lane (r0 + lane and
+// r0 + 32 + lane), for tiles without sticky states: both table lookups of a
+// lane are issued before either list is read, so a warp has two lookups in
+// flight per lane. Same entries and reports as inject_aas over the two halves.
+__device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                            const TileView& tv, const UnitCtx& c, int lane, int r0,
+                                            int batch, int depth, unsigned long long& n_injected) {
+  const TileDev& t = *tv.t;
+  int k[2], kmax[2], r[2];
+  uint32_t key[2], vb[2], ve[2];
+  bool valid[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    r[h] = r0 + 32 * h + lane;
+    valid[h] = 32 * h + lane < batch && r[h] < c.iend;
+    kmax[h] = valid[h] ? min(depth, c.wlen - r[h]) : 0;
+    k[h] = kmax[h];
+    key[h] = 0u;
+    for (int d = 0; d < depth; d++) {
+      if (d < k[h]) {
+        const uint32_t sym = c.in[r[h] + d];
+        if (sym >= tv.nlive) k[h] = d;
+        else key[h] = key[h] * tv.nlive + sym;
+      }
+    }
+    vb[h] = ve[h] = 0u;
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    if (k[h] == kmax[h] && k[h] > 0) {
+      uint32_t rb, re;
+      pt_find(tv.pt[k[h] - 1], key[h], true, false, vb[h], ve[h], rb, re);
+    }
+  }
+  if (tv.rep_levels) {  // reports of the first k symbols, level by level
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int64_t q = c.wb + r[h];
+      uint32_t kk = 0;
+      for (int d = 0; d < depth; d++) {
+        const bool act = d < k[h];
+        if (act) kk = kk * tv.nlive + c.in[r[h] + d];
+        if (!((tv.rep_levels >> d) & 1u)) continue;
+        const PrefixTableDev& pt = tv.pt[d];
+        uint32_t b0, e0, rb, re;
+        pt_find(pt, kk, false, act, b0, e0, rb, re);
+        const int len = (int)(re - rb);
+        const int mx = __reduce_max_sync(kFull, len);
+        for (int i = 0; i < mx; i++) {
+          const bool ok = i < len && q + d >= c.emit_lo;
+          const uint32_t v = ok ? __ldg(pt.rlist + rb + i) : 0u;
+          emit_report(p, ws, w, lane, ok, ok ? (__ldg(t.sid + v)) : 0u, (uint32_t)(q + d));
+        }
+      }
+    }
+  }
+  // entries at the unit's last position have nothing to expand
+  uint32_t len[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    len[h] = (k[h] == kmax[h] && k[h] > 0 && c.wb + r[h] + k[h] < c.hi) ? (ve[h] - vb[h]) : 0u;
+    n_injected += len[h];
+  }
+  const uint32_t mine = len[0] + len[1];
+  uint32_t incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  if (__reduce_max_sync(kFull, max(len[0], len[1])) <= 4u) {
+    // short lists: every lane copies its own two
+    uint32_t pos = incl - mine;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uint32_t off = (uint32_t)(r[h] + k[h] - 1);
+      const uint32_t* vl = tv.pt[(k[h] > 0 ? k[h] : 1) - 1].vlist;
+      for (uint32_t j = 0; j < len[h]; j++)
+        store_entry(p, ws, w, w.top + (int)(pos + j),
+                    (__ldg(vl + vb[h] + j) << kEntryPosBits) | off);
+      pos += len[h];
+    }
+    grow_stack(p, w, (int)total);
+    __syncwarp();
+    return;
+  }
+  // long lists: the two halves one after the other, each copied cooperatively
+  int base = w.top;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    uint32_t hi = len[h];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, hi, o);
+      if (lane >= o) hi += y;
+    }
+    const uint32_t ht = __shfl_sync(kFull, hi, 31);
+    ws.inj[lane] = hi;
+    ws.inj[32 + lane] = vb[h];
+    ws.inj[64 + lane] = (uint32_t)(k[h] > 0 ? k[h] : 1);
+    __syncwarp();
+    for (uint32_t idx = lane; idx < ht; idx += 32) {
+      int l0 = 0, l1 = 31;
+      while (l0 < l1) {  // first lane whose inclusive prefix exceeds idx
+        const int m = (l0 + l1) >> 1;
+        if (ws.inj[m] > idx) l1 = m;
+        else l0 = m + 1;
+      }
+      const uint32_t before = l0 > 0 ? ws.inj[l0 - 1] : 0u;
+      const int kk = (int)ws.inj[64 + l0];
+      const uint32_t v = __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
+      const uint32_t off = (uint32_t)(r0 + 32 * h + l0 + kk - 1);
+      store_entry(p, ws, w, base + (int)idx, (v << kEntryPosBits) | off);
+    }
+    base += (int)ht;
+    __syncwarp();
+  }
+  grow_stack(p, w, (int)total);
+  __syncwarp();
+}
+
 // Injection of a batch of positions: always-active states, then the sticky
 // states met while copying, then the work of every active sticky state at
 // these positions. Layered tiles (phase 2) do their sticky work separately.
@@ -781,18 +927,21 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
   const int64_t q = c.wb + r;
   const bool go = e != kNoEntry && q + 1 < c.hi;
   uint4 sc = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+  uint4 sm = make_uint4(0u, 0u, 0u, 0u);
   uint32_t s = 0;
   if (go) {
     sc = load_succ(tv, v);
+    if (tv.fused) sm = load_smask(tv, v);
     s = c.in[r + 1];
   }
   n_expanded += go;
   const uint32_t u[4] = {sc.x, sc.y, sc.z, sc.w};
+  const uint32_t um[4] = {sm.x, sm.y, sm.z, sm.w};
   bool ok[4];
   int cnt = 0;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    ok[j] = go && u[j] != kNoSucc && accepts(tv, u[j] & kIdMask, s);
+    ok[j] = go && succ_accepts(tv, u[j], um[j], s);
     cnt += ok[j];
   }
   report4(p, ws, w, tv, lane, ok, u, q + 1, q + 1 >= c.emit_lo);
@@ -841,14 +990,19 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     uint4 sc2 = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
-    if (inner && ok[j]) sc2 = load_succ(tv, u[j] & kIdMask);
+    uint4 sm2 = make_uint4(0u, 0u, 0u, 0u);
+    if (inner && ok[j]) {
+      sc2 = load_succ(tv, u[j] & kIdMask);
+      if (tv.fused) sm2 = load_smask(tv, u[j] & kIdMask);
+    }
     u2[j][0] = sc2.x;
     u2[j][1] = sc2.y;
     u2[j][2] = sc2.z;
     u2[j][3] = sc2.w;
+    const uint32_t um2[4] = {sm2.x, sm2.y, sm2.z, sm2.w};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      ok2[j][k] = u2[j][k] != kNoSucc && accepts(tv, u2[j][k] & kIdMask, s2);
+      ok2[j][k] = succ_accepts(tv, u2[j][k], um2[k], s2);
       cnt2 += ok2[j][k];
     }
   }
@@ -874,6 +1028,85 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
 #pragma unroll
       for (int k = 0; k < 4; k++)
         if (ok2[j][k]) store_entry(p, ws, w, pos++, ((u2[j][k] & kIdMask) << kEntryPosBits) | tag);
+  }
+  grow_stack(p, w, total);
+  __syncwarp();
+}
+
+// One worklist step over up to 64 entries, two per lane, for tiles without
+// sticky states and without privatization: both entries' successor records
+// are requested before either is used, so a warp keeps two L2 round trips in
+// flight per lane instead of one. Same results as two expand_step calls.
+__device__ __forceinline__ void expand_step2(const MatchParams& p, WarpSmem& ws, WarpRun& w,
+                                             const TileView& tv, const UnitCtx& c, int lane,
+                                             unsigned long long& n_expanded) {
+  const int n = min(w.top, 64);
+  uint32_t e[2];
+  e[0] = lane < n ? ws.stack[w.top - 1 - lane] : kNoEntry;
+  e[1] = lane + 32 < n ? ws.stack[w.top - 33 - lane] : kNoEntry;
+  w.top -= n;
+  __syncwarp();
+  if (p.unique) {  // identical entries in one half-step are expanded once (--unique)
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const unsigned peers = __match_any_sync(kFull, e[k]);
+      if ((__ffs(peers) - 1) != lane) e[k] = kNoEntry;
+    }
+  }
+  uint4 sc[2], sm[2];
+  uint32_t s[2];
+  int r[2];
+  bool go[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    r[k] = (int)(e[k] & ((1u << kEntryPosBits) - 1));
+    go[k] = e[k] != kNoEntry && c.wb + r[k] + 1 < c.hi;
+    sc[k] = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+    sm[k] = make_uint4(0u, 0u, 0u, 0u);
+    s[k] = 0u;
+    if (go[k]) {
+      const uint32_t v = e[k] >> kEntryPosBits;
+      sc[k] = load_succ(tv, v);
+      if (tv.fused) sm[k] = load_smask(tv, v);
+      s[k] = c.in[r[k] + 1];
+    }
+    n_expanded += go[k];
+  }
+  bool ok[2][4], need[2], at_end[2];
+  int cnt = 0;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const uint32_t u[4] = {sc[k].x, sc[k].y, sc[k].z, sc[k].w};
+    const uint32_t um[4] = {sm[k].x, sm[k].y, sm[k].z, sm[k].w};
+    const int64_t q = c.wb + r[k];
+#pragma unroll
+    for (int j = 0; j < 4; j++) ok[k][j] = go[k] && succ_accepts(tv, u[j], um[j], s[k]);
+    report4(p, ws, w, tv, lane, ok[k], u, q + 1, q + 1 >= c.emit_lo);
+    need[k] = go[k] && q + 2 < c.hi;
+    at_end[k] = r[k] + 1 == c.wlen;
+    if (__any_sync(kFull, need[k] && at_end[k])) {
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        carry_state(p, w, lane, need[k] && at_end[k] && ok[k][j], u[j] & kIdMask);
+    }
+    if (need[k] && !at_end[k]) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) cnt += ok[k][j];
+    }
+  }
+  int total;
+  const int ex = warp_excl<4>(cnt, lane, total);
+  if (cnt) {
+    int pos = w.top + ex;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      if (!(need[k] && !at_end[k])) continue;
+      const uint32_t u[4] = {sc[k].x, sc[k].y, sc[k].z, sc[k].w};
+      const uint32_t tag = (uint32_t)(r[k] + 1);
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (ok[k][j]) store_entry(p, ws, w, pos++, ((u[j] & kIdMask) << kEntryPosBits) | tag);
+    }
   }
   grow_stack(p, w, total);
   __syncwarp();
@@ -980,11 +1213,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     tv.pt = s_pt;
     tv.cw = t->cw;
     tv.narrow = t->narrow;
+    tv.fused = t->fused;
     tv.nlive = (uint32_t)t->nlive;
     tv.rep_levels = 0u;
     for (int d = 0; d < kMaxDepth; d++) tv.rep_levels |= (s_pt[d].has_reports ? 1u : 0u) << d;
     const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
     const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
+    // short table lists, no sticky states: two positions per lane per injection
+    const bool wide_inject = depth > 0 && !tv.sticky && batch == 32;
     const bool translate = t->cw != 8;
     // Without sticky states registered during the window (plain tiles
     // without them, layered tiles), the last depth - 1 positions of a window
@@ -1053,14 +1289,19 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       }
       int cur = 0;
       uint32_t nbytes[2], skip[2];
-      nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
+      if ((int32_t)uid != p.skip_copy_unit) {
+        nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
+      } else {  // test hook: nothing is in flight, the first wait gives up
+        nbytes[0] = 0u;
+        skip[0] = 0u;
+      }
       int64_t inj_pos = un.lo;  // next position for always-active injection
       for (int64_t wb = un.lo; wb < c.hi; wb += W) {
         const int64_t we = min(wb + (int64_t)W, c.hi);
         c.wb = wb;
         c.wlen = (int)(we - wb);
         c.iend = we == c.hi ? c.wlen : c.wlen - defer;
-        if (!mbar_wait(&ws.bar[cur], phase[cur])) {
+        if (!mbar_wait(&ws.bar[cur], phase[cur], p.wait_rounds)) {
           if (lane == 0) atomicOr(p.err, kErrTimeout);
           dead = true;
           break;
@@ -1116,8 +1357,13 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
           // most one batch's excess
           if (w.top < kInjectLow && w.ovf_n == 0) {
             if (cursor < c.iend) {
-              inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
-              cursor += batch;
+              if (wide_inject) {
+                inject_aas2(p, ws, w, tv, c, lane, cursor, 2 * batch, depth, n_injected);
+                cursor += 2 * batch;
+              } else {
+                inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
+                cursor += batch;
+              }
               continue;
             }
             if (scur < c.wlen) {
@@ -1138,7 +1384,10 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
             if (cursor < c.iend || scur < c.wlen) continue;
             break;
           }
-          expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
+          if (PRIV == 0 && !tv.sticky)
+            expand_step2(p, ws, w, tv, c, lane, n_expanded);
+          else
+            expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
         }
         inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
         cur ^= 1;
@@ -1155,7 +1404,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         // wait (bounded) for any copy still in flight before giving up on this warp
         for (int b = 0; b < 2; b++)
           if (pending[b]) {
-            mbar_wait(&ws.bar[b], phase[b]);
+            mbar_wait(&ws.bar[b], phase[b], p.wait_rounds);
             pending[b] = false;
           }
         __syncwarp();

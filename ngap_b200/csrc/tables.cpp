@@ -383,7 +383,10 @@ void build_image(TileHost& t) {
   auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
   const size_t n = (size_t)t.nstates;
   t.narrow = t.nstates <= kNarrowMaxStates;
-  t.off_cmask = (int32_t)r16(n * (t.narrow ? 8 : 16));
+  // wide tiles are read through L2: with one class word, a state's record also
+  // carries its successors' class masks, so that an expansion is one round trip
+  t.fused = !t.narrow && t.cw == 1;
+  t.off_cmask = (int32_t)r16(n * (t.narrow ? 8 : (t.fused ? 32 : 16)));
   t.off_rep = t.off_cmask + (int32_t)r16(n * t.cw * 4);
   t.off_sticky = t.off_rep + (int32_t)r16(((n + 31) / 32) * 4);
   t.off_cls = t.off_sticky + (int32_t)r16(((n + 31) / 32) * 4);
@@ -395,6 +398,14 @@ void build_image(TileHost& t) {
       s16[i] = u == kNoSucc ? (uint16_t)0xffff
                             : (uint16_t)((u & 0x7fffu) | ((u >> 31) ? 0x8000u : 0u));
     }
+  } else if (t.fused) {  // [4 x u32 successor][4 x u32 its class mask, 0 = none] per state
+    uint32_t* rec = reinterpret_cast<uint32_t*>(t.image.data());
+    for (size_t i = 0; i < n; i++)
+      for (int j = 0; j < 4; j++) {
+        const uint32_t u = t.succ[i * 4 + j];
+        rec[i * 8 + j] = u;
+        rec[i * 8 + 4 + j] = u == kNoSucc ? 0u : t.cmask[(size_t)(u & 0x7fffffffu)];
+      }
   } else {
     memcpy(t.image.data(), t.succ.data(), n * 16);
   }

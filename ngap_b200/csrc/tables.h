@@ -26,6 +26,8 @@ struct TileHost {
   int32_t num_ccs = 0;
   int32_t ncls = 0, cw = 8, nlive = 0;
   bool narrow = true;                // 16-bit successor ids in the image
+  bool fused = false;                // wide tile of <= 32 classes: each state's successor ids and
+                                     // their class masks in one 32-byte record
   int32_t inj_batch = 32;            // positions injected per worklist refill
   int32_t inj_batch0 = 32;           // the same without prefix tables (AAS scan)
   bool global = false;               // tables read through L2, never staged in shared memory

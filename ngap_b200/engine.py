@@ -280,6 +280,13 @@ class Engine:
     def device_bytes(self):
         return lib().ngap_engine_device_bytes(self._h)
 
+    def memory(self):
+        """Device bytes the engine holds, by part: dict with input, reports,
+        scratch (per-warp worklist scratch) and plan."""
+        m = _lib.EngineMem()
+        check(lib().ngap_engine_memory(self._h, ctypes.byref(m)))
+        return {k: getattr(m, k) for k in ("input", "reports", "scratch", "plan")}
+
     def match(self, tables, data, num_seg, seg_len, **kw):
         """match_async, sync and results: sorted unique reports (uint64)."""
         self.match_async(tables, data, num_seg, seg_len, **kw)

@@ -39,6 +39,19 @@ def _noalloc(torch, d_in, n, d_out):
     return nout.value
 
 
+def _host_unique(rep):
+    """numpy sort by (offset, id) and unique, in the reference encoding."""
+    key = ((rep & np.uint64(0xFFFFFFFF)) << np.uint64(32)) | (rep >> np.uint64(32))
+    uk = np.unique(key)
+    return (uk << np.uint64(32)) | (uk >> np.uint64(32))
+
+
+def _exact(seed, n):
+    """Exactly n reports (about a third of them duplicates)."""
+    rep = _reports(seed, max(1, (3 * n) // 4 + 1))
+    return np.resize(rep, n)
+
+
 def test_noalloc_matches_sort_unique(engine):
     import torch
     for seed, n in ((1, 150_000), (2, 60_000)):  # two calls in a row, different sizes
@@ -56,10 +69,36 @@ def test_noalloc_matches_sort_unique(engine):
         want = d_ref[:n_ref].cpu().numpy().view(np.uint64)
         assert np.array_equal(got, want)
         # and against a host sort by (offset, id) + unique
-        key = ((rep & np.uint64(0xFFFFFFFF)) << np.uint64(32)) | (rep >> np.uint64(32))
-        uk = np.unique(key)
-        host = (uk << np.uint64(32)) | (uk >> np.uint64(32))
-        assert np.array_equal(got, host)
+        assert np.array_equal(got, _host_unique(rep))
+
+
+@pytest.mark.parametrize("n", [1, 2047, 2049, MAX_REPORTS])
+def test_noalloc_edge_sizes(engine, n):
+    """One report, either side of a 2048-key sort tile, and the full scratch."""
+    import torch
+    rep = _exact(10 + n, n)
+    assert len(rep) == n
+    d_in = torch.from_numpy(rep.view(np.int64)).cuda()
+    d_out = torch.full_like(d_in, -1)
+    n_new = _noalloc(torch, d_in, n, d_out)
+    d_ref = torch.empty_like(d_in)
+    n_ref = engine.sort_unique_device(d_in.data_ptr(), n, d_ref.data_ptr(),
+                                      stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    got = d_out[:n_new].cpu().numpy().view(np.uint64)
+    assert n_new == n_ref and np.array_equal(got, d_ref[:n_ref].cpu().numpy().view(np.uint64))
+    assert np.array_equal(got, _host_unique(rep))
+
+
+def test_noalloc_in_place(engine):
+    """d_out may be d_in: the input is read into the scratch before any pass
+    writes the output."""
+    import torch
+    rep = _reports(21, 90_000)
+    d = torch.from_numpy(rep.view(np.int64)).cuda()
+    n_new = _noalloc(torch, d, len(rep), d)
+    torch.cuda.synchronize()
+    assert np.array_equal(d[:n_new].cpu().numpy().view(np.uint64), _host_unique(rep))
 
 
 def test_noalloc_rejects_oversize(engine):
