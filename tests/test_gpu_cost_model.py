@@ -57,6 +57,113 @@ def test_feature_kernel_matches_host_definition(small_suite):
         assert np.allclose(got[i], want, atol=1e-5), i
 
 
+H = 64
+
+
+def _unpack(p, D):
+    """W1[D][H], b1[H], W2[H][H], b2[H], w3[H], b3 from the flat parameter
+    vector (the layout of ngap_mlp_get_params)."""
+    o = 0
+    W1 = p[o:o + D * H].reshape(D, H); o += D * H
+    b1 = p[o:o + H]; o += H
+    W2 = p[o:o + H * H].reshape(H, H); o += H * H
+    b2 = p[o:o + H]; o += H
+    w3 = p[o:o + H]; o += H
+    return W1, b1, W2, b2, w3, p[o]
+
+
+def _np_forward(p, x, D, rnd=lambda a: a):
+    W1, b1, W2, b2, w3, b3 = (rnd(a) for a in _unpack(p, D))
+    h1 = rnd(np.maximum(rnd(x) @ W1 + b1, 0.0))
+    h2 = rnd(np.maximum(h1 @ W2 + b2, 0.0))
+    return h2 @ w3 + b3, h1, h2
+
+
+def _bf16(a):
+    """Round float32 values to bfloat16 (round to nearest, ties to even),
+    returned as float64."""
+    u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+def _model(D, seed):
+    m = cm.LearnedModel(0, seed=seed, in_dim=D)
+    rng = np.random.default_rng(seed)
+    p = (rng.standard_normal(len(m.params())) * 0.2).astype(np.float32)
+    m.set_params(p)
+    return m, p.astype(np.float64), rng
+
+
+def _raw_predict(m, x, bf16):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros(len(x), np.float32)
+    nb.lib().ngap_mlp_predict(m._h, x.ctypes.data, len(x), int(bf16), out.ctypes.data)
+    return out.astype(np.float64)
+
+
+def test_mlp_fp32_forward_matches_numpy():
+    """mlp_infer_kernel<false> against a float64 numpy forward pass of the
+    same parameters: relative tolerance 1e-5 (FP32 accumulation of at most
+    266 products in a different order)."""
+    D = cm.IN_DIM
+    m, p, rng = _model(D, 5)
+    x = rng.standard_normal((333, D)).astype(np.float32)  # a partial last block of rows
+    want, _, _ = _np_forward(p, x.astype(np.float64), D)
+    got = _raw_predict(m, x, bf16=False)
+    scale = np.abs(want).max()
+    assert np.allclose(got, want, rtol=1e-5, atol=1e-5 * scale)
+
+
+def test_mlp_bf16_forward_matches_numpy_rounding():
+    """mlp_infer_kernel<true> rounds inputs, weights and activations to bfloat16
+    and accumulates in FP32: against a numpy forward pass with the same
+    roundings (float64 accumulation), tolerance 4e-3 of the largest output
+    (an activation whose FP32 sum lies within one bfloat16 step of a rounding
+    boundary may round the other way, 2^-8 of it), and within 5 % of the FP32
+    result."""
+    D = cm.IN_DIM
+    m, p, rng = _model(D, 6)
+    x = rng.standard_normal((256, D)).astype(np.float32)
+    want, _, _ = _np_forward(p, x.astype(np.float64), D, rnd=_bf16)
+    got = _raw_predict(m, x, bf16=True)
+    scale = np.abs(want).max()
+    assert np.allclose(got, want, rtol=4e-3, atol=4e-3 * scale)
+    fp32, _, _ = _np_forward(p, x.astype(np.float64), D)
+    assert np.abs(got - fp32).max() <= 0.05 * np.abs(fp32).max()
+
+
+def test_mlp_gradient_matches_numpy_backprop():
+    """mlp_grad_kernel (the gradient that ngap_mlp_train gives to Adam)
+    against float64 numpy backpropagation of the mean squared error:
+    relative tolerance 1e-4 of the largest gradient entry (FP32 sums and
+    atomic accumulation across blocks in any order)."""
+    D = 40
+    m, p, rng = _model(D, 7)
+    n = 300
+    x = rng.standard_normal((n, D)).astype(np.float32)
+    t = rng.standard_normal(n).astype(np.float32)
+    grad = np.zeros(len(p), np.float32)
+    loss = np.zeros(1, np.float32)
+    import ctypes
+    rc = nb.lib().ngap_mlp_gradient(m._h, x.ctypes.data, t.ctypes.data, n, grad.ctypes.data,
+                                     ctypes.cast(loss.ctypes.data, ctypes.POINTER(ctypes.c_float)))
+    assert rc == 0
+    X = x.astype(np.float64)
+    y, h1, h2 = _np_forward(p, X, D)
+    W1, b1, W2, b2, w3, b3 = _unpack(p, D)
+    dy = 2.0 * (y - t) / n
+    d2 = (h2 > 0) * np.outer(dy, w3)
+    d1 = (h1 > 0) * (d2 @ W2.T)
+    want = np.concatenate([(X.T @ d1).ravel(), d1.sum(0), (h1.T @ d2).ravel(), d2.sum(0),
+                           h2.T @ dy, [dy.sum()]])
+    g = grad.astype(np.float64)
+    assert np.allclose(g, want, rtol=1e-4, atol=1e-4 * np.abs(want).max())
+    assert np.isclose(loss[0], np.mean((y - t) ** 2), rtol=1e-4)
+    # the parameters are unchanged by the gradient call
+    assert np.array_equal(m.params(), p.astype(np.float32))
+
+
 def test_mlp_trains_and_bf16_follows_fp32():
     rng = np.random.default_rng(3)
     x = rng.standard_normal((4000, 20)).astype(np.float32)
@@ -112,10 +219,11 @@ def test_serving_results_same_alone_and_in_the_mix(engine, small_suite):
     for name, pred in (("default", None), ("static", sv.Predictor("static", tables)),
                        ("learned", sv.Predictor("learned", tables, lm))):
         rs = [sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in reqs]
-        srv = sv.Server(ts, predictor=pred, slots=2, budget=1 << 22, max_batch_bytes=1 << 20,
+        srv = sv.Server(ts, predictor=pred, slots=2, budget=4 << 30, max_batch_bytes=1 << 20,
                         queue_capacity=cm.queue_for(4.0) if pred else 0)
         m = srv.run(rs)
         assert m["requests"] == len(reqs) and m["p99_ms"] >= m["p50_ms"] > 0
+        assert m["rejected"] == 0 and srv.held_bytes() <= srv.budget
         served[name] = rs
     for r in reqs:
         want, _ = oracle.match(groups[r.nfa].views(), r.data, 1, len(r.data))
