@@ -8,6 +8,7 @@
 // C ABI; --validation runs the library's CPU checker as the reference does.
 #include <algorithm>
 #include <cctype>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -229,6 +230,120 @@ bool dump_reports(const std::string& path, const std::vector<uint64_t>& v) {
   return true;
 }
 
+// --tuning (ngap.cu:1995-2056): the reference reruns the whole input over a
+// grid of its knobs (fetch size x AAS interval x active threshold) and keeps
+// the fastest run that validates. The knobs here are the engine's: window,
+// chunk length and, for the privatizing algorithms, the active threshold. A
+// candidate counts only when its reports equal the first candidate's. The
+// best choice is written back into mp for the run that follows.
+bool tune(ngap_engine* eng, const ngap_tables* tables, const std::vector<uint8_t>& ss,
+          uint64_t total, ngap_match_params& mp) {
+  const bool priv = mp.algorithm == NGAP_ALGO_NONBLOCKING_R1 ||
+                    mp.algorithm == NGAP_ALGO_NONBLOCKING_R2 ||
+                    mp.algorithm == NGAP_ALGO_NONBLOCKING_ALL;
+  const std::vector<int> windows{256, 512, 1024, 2048, 4096};
+  const std::vector<int> chunks{0, 4096, 16384};
+  const std::vector<int> thresholds =
+      priv ? std::vector<int>{0, 8, 16, 24, 32} : std::vector<int>{mp.active_threshold};
+  std::vector<uint64_t> base;
+  bool have_base = false;
+  double best_thr = -1;
+  int best[3] = {mp.window, mp.chunk, mp.active_threshold};
+  const auto t_all = std::chrono::steady_clock::now();
+  for (int w : windows)
+    for (int th : thresholds)
+      for (int ch : chunks) {
+        const auto t0 = std::chrono::steady_clock::now();
+        printf("[Tuning] Try choice: \n   window=%d, chunk=%d, active_threshold=%d\n", w, ch, th);
+        ngap_match_params m = mp;
+        m.window = w;
+        m.chunk = ch;
+        m.active_threshold = th;
+        int rc = ngap_match(eng, tables, ss.data(), 0, &m, nullptr);
+        if (rc == NGAP_OK) rc = ngap_engine_sync(eng);
+        bool pass = rc == NGAP_OK;
+        double thr = -1;
+        if (pass) {
+          float a = 0, b = 0;
+          ngap_last_times_ms(eng, &a, &b);
+          thr = (double)total / (((double)a + (double)b) * 1000.0);
+          if (!m.report_off) {
+            uint64_t raw = 0, uniq = 0;
+            ngap_results_count(eng, &raw, &uniq);
+            std::vector<uint64_t> res(uniq);
+            if (uniq) ngap_results_copy(eng, res.data(), uniq);
+            if (!have_base) {
+              base.swap(res);
+              have_base = true;
+            } else {
+              pass = res == base;
+            }
+          }
+        }
+        if (pass && thr > best_thr) {
+          best_thr = thr;
+          best[0] = w;
+          best[1] = ch;
+          best[2] = th;
+          printf("[Tuning] Update best choice: \n   window=%d, chunk=%d, active_threshold=%d "
+                 "max_throughput=%f\n", best[0], best[1], best[2], best_thr);
+        } else {
+          printf("[Tuning] Keep best choice: \n   window=%d, chunk=%d, active_threshold=%d "
+                 "max_throughput=%f\n", best[0], best[1], best[2], best_thr);
+        }
+        const double sec =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::cout << "[Tuning] " << sec << " seconds\n";
+      }
+  const double all =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t_all).count();
+  std::cout << "[Tuning] Total time: " << all << " seconds\n";
+  if (best_thr < 0) {
+    std::cout << "ERROR: no tuning choice ran: " << err_msg() << std::endl;
+    return false;
+  }
+  printf("[Tuning] Tuning completed: the best choice is\n   window=%d, chunk=%d, "
+         "active_threshold=%d\n", best[0], best[1], best[2]);
+  mp.window = best[0];
+  mp.chunk = best[1];
+  mp.active_threshold = best[2];
+  return true;
+}
+
+// --motivate-worklist-length (ngap.cu:1843-1866): the reference appends the
+// worklist length fetched per round to a file named after --app-name. The
+// engine has no global rounds; it records each unit's worklist work (entries
+// expanded plus entries injected by the warp that matched one tile over one
+// chunk of a segment), written one unit per line: segment, tile, first and
+// last position (relative to the segment), work.
+bool save_worklist(ngap_engine* eng, const std::string& app_name) {
+  int64_t n = 0;
+  if (ngap_trace_copy(eng, nullptr, 0, &n) != NGAP_OK) {
+    std::cout << "ERROR: " << err_msg() << std::endl;
+    return false;
+  }
+  std::vector<ngap_unit_trace> tr((size_t)std::max<int64_t>(n, 1));
+  if (n > 0 && ngap_trace_copy(eng, tr.data(), n, &n) != NGAP_OK) {
+    std::cout << "ERROR: " << err_msg() << std::endl;
+    return false;
+  }
+  const std::string path = (app_name.empty() ? std::string("ngap") : app_name) + ".worklist.txt";
+  printf("Save froniter length file to %s\n", path.c_str());
+  FILE* f = fopen(path.c_str(), "w");
+  if (!f) {
+    std::cerr << "Error: cannot open " << path << " for writing" << std::endl;
+    return false;
+  }
+  for (int64_t i = 0; i < n; i++)
+    fprintf(f, "%d %d %lld %lld %llu\n", tr[i].stream, tr[i].tile, (long long)tr[i].lo,
+            (long long)tr[i].hi, (unsigned long long)tr[i].work);
+  if (fclose(f) != 0) {
+    std::cerr << "Error: writing " << path << " failed" << std::endl;
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -340,12 +455,15 @@ int main(int argc, char** argv) {
   mp.window = o.window;
   mp.chunk = o.chunk;
   const uint64_t total = (uint64_t)num_seg * (uint64_t)seg_len;
+  if (o.tuning && !tune(eng, tables, ss, total, mp)) return 255;
+  if (o.motivate_worklist_length) ngap_engine_set_trace(eng, 1);
   int rc = ngap_match(eng, tables, ss.data(), 0, &mp, nullptr);
   if (rc == NGAP_OK) rc = ngap_engine_sync(eng);
   if (rc != NGAP_OK && rc != NGAP_E_OVERFLOW_RESULTS) {
     std::cout << "ERROR: " << err_msg() << std::endl;
     return 255;
   }
+  if (o.motivate_worklist_length && !save_worklist(eng, o.app_name)) return 255;
   float match_ms = 0, sort_ms = 0;
   ngap_last_times_ms(eng, &match_ms, &sort_ms);
   const double ms = (double)match_ms + (double)sort_ms;
