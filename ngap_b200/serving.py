@@ -11,16 +11,18 @@ single 1 MB input. Here:
   from the queued requests and launches it with ngap_batch_match, so that
   requests arriving while others run are admitted as slots and memory free
   up, and batches on different slots overlap on the device;
-* admission: a batch is launched only while the input bytes held by
-  in-flight batches stay within `budget` bytes of device memory (each
-  engine's report buffers are sized once, for `max_batch_bytes`);
-* batches take the queue in arrival order; the scheduler sets each
-  request's chunk length from its predicted density (cost_model.chunk_for:
-  a unit's serial time bounds a batch's latency, so requests predicted
-  denser than rho_ref get proportionally shorter chunks, never longer than
-  chunk_hi) and the queue capacity from the densest prediction; "default"
-  uses the engine's fixed chunks, "static" the table rule's prediction,
-  "learned" the MLP's;
+* admission: the tables and every engine's buffers (input copy, report
+  buffers, per-warp overflow stacks, unit plan) count against `budget` bytes
+  of device memory; a batch is launched only when what it adds keeps the
+  total within the budget, and a request that can never fit is rejected
+  with an error instead of waiting forever;
+* batches take the queue in arrival order; with a predictor, each request's
+  work is predicted at arrival (density x length; "static" is the table
+  rule's density, "learned" the MLP's on the request's own bytes) and can
+  set its chunk length (cost_model.chunk_for: requests predicted denser than
+  rho_ref get proportionally shorter chunks) and, with `isolate`, its lane:
+  predicted-heavy requests are batched apart from the light ones, so a light
+  request never waits for a heavy batch (Server.run);
 * each request's reports are exactly those of matching it alone
   (tests/test_gpu_cost_model.py checks this for every scheduler).
 """
@@ -44,6 +46,7 @@ class Request:
     chunk: int = 0                  # chunk length for the request's stream (0 = default)
     done: float = -1.0              # completion time (seconds from the start)
     reports: np.ndarray = field(default=None, repr=False)
+    error: str = None               # set when the request can never be admitted
 
 
 def make_requests(pool, nfa_of_stream, n_nfas, rate=2000.0, duration=2.0, median=64 << 10,
@@ -122,43 +125,26 @@ class Predictor:
         return self.model.predict(nf, x, bf16=True)
 
 
-class Server:
-    """Continuous batching over `slots` engines sharing one tableset."""
+class EngineSlot:
+    """One engine on its own non-blocking CUDA stream with a pinned staging
+    buffer: the unit the server launches batches on."""
 
-    def __init__(self, tableset, predictor=None, rho_ref=2.0, slots=2, budget=1 << 30,
-                 max_batch_bytes=64 << 20, device=0, queue_capacity=0,
-                 algorithm="nonblockingpcgroups", base_chunk=2048, chunk_lo=256, chunk_hi=2048):
+    def __init__(self, tableset, device, max_batch_bytes):
         import torch
         from .engine import Engine
         self.torch = torch
         self.ts = tableset
-        self.pred = predictor
-        self.rho_ref = rho_ref
-        self.base_chunk = base_chunk
-        self.chunk_lo, self.chunk_hi = chunk_lo, chunk_hi
-        self.budget = budget
-        self.max_bytes = max_batch_bytes
-        self.queue_capacity = queue_capacity
-        self.algorithm = algorithm
-        self.engines = [Engine(device) for _ in range(slots)]
-        self.streams = [torch.cuda.Stream(device) for _ in range(slots)]
-        self.pinned = [torch.empty(max_batch_bytes, dtype=torch.uint8).pin_memory()
-                       for _ in range(slots)]
-        self.rep_cap = max(1 << 16, max_batch_bytes // 4)
-        self.busy = [None] * slots      # (batch, event, held bytes, launch arguments)
-        self.batches = []               # (size, bytes, predicted work, device ms)
-        self.launches = 0               # kernels launched by the served batches
+        self.engine = Engine(device)
+        self.stream = torch.cuda.Stream(device)
+        self.pinned = torch.empty(max_batch_bytes, dtype=torch.uint8).pin_memory()
+        self.event = None
+        self.args = None
 
-    def _held(self):
-        return sum(b[2] for b in self.busy if b is not None)
+    def memory(self):
+        return self.engine.memory()
 
-    def _reserve(self, nbytes):
-        """Device bytes a batch holds while in flight: its input (the report
-        buffers are sized once per engine, `rep_cap` reports)."""
-        return nbytes
-
-    def _launch(self, slot, batch):
-        buf = self.pinned[slot].numpy()
+    def launch(self, batch, params):
+        buf = self.pinned.numpy()
         offs = np.zeros(len(batch), np.int64)
         lens = np.array([len(r.data) for r in batch], np.int64)
         pos = 0
@@ -167,84 +153,208 @@ class Server:
             buf[pos:pos + len(r.data)] = r.data
             pos += len(r.data)
         nfa = np.array([r.nfa for r in batch], np.int32)
-        eng, st = self.engines[slot], self.streams[slot]
-        kw = dict(algorithm=self.algorithm, result_capacity=self.rep_cap,
-                  stream=st.cuda_stream, queue_capacity=self.queue_capacity,
+        kw = dict(params, stream=self.stream.cuda_stream,
                   chunks=np.array([r.chunk for r in batch], np.int64))
-        batch_match_async(eng, self.ts, buf[:pos], offs, lens, nfa, **kw)
-        ev = self.torch.cuda.Event()
-        ev.record(st)
-        self.busy[slot] = (batch, ev, self._reserve(pos), (offs, lens, nfa, kw, pos))
+        batch_match_async(self.engine, self.ts, buf[:pos], offs, lens, nfa, **kw)
+        self.event = self.torch.cuda.Event()
+        self.event.record(self.stream)
+        self.args = (offs, lens, nfa, kw, pos)
 
-    def _finish(self, slot, now):
-        batch, ev, held, (offs, lens, nfa, kw, pos) = self.busy[slot]
-        eng = self.engines[slot]
+    def done(self):
+        return self.event.query()
+
+    def finish(self, nreq):
+        """Waits for the batch; (per-request reports, device ms, kernel launches)."""
+        offs, lens, nfa, kw, pos = self.args
+        eng = self.engine
         try:
             eng.sync()
         except NgapError as ex:  # capacity exceeded: rerun with the defaults (same reports)
             if ex.status not in (6, 7):
                 raise
             kw = dict(kw, queue_capacity=0, result_capacity=max(kw["result_capacity"] * 8, 8 * pos))
-            batch_match_async(eng, self.ts, self.pinned[slot].numpy()[:pos], offs, lens, nfa, **kw)
+            batch_match_async(eng, self.ts, self.pinned.numpy()[:pos], offs, lens, nfa, **kw)
             eng.sync()
-        dev_ms = sum(eng.times_ms())
-        self.launches += eng.launches()
         reps, sids = batch_results(eng)
-        per = split_by_stream(reps, sids, len(batch))
-        t = time.perf_counter() - self._t0
-        for r, rep in zip(batch, per):
-            r.reports = rep
-            r.done = t
-        self.batches.append((len(batch), pos, sum(r.pred_work for r in batch), dev_ms))
-        self.busy[slot] = None
+        return split_by_stream(reps, sids, nreq), sum(eng.times_ms()), eng.launches()
 
-    def _form(self, queue):
-        """Requests for the next batch, in arrival order, while the batch fits
-        max_batch_bytes and the in-flight bytes fit the budget (removed from
+
+def padded_input(nbytes):
+    """Bytes of an engine's input copy for a batch of nbytes (16-byte padded + 64)."""
+    return ((int(nbytes) + 15) & ~15) + 64
+
+
+class Server:
+    """Continuous batching over `slots` engines sharing one tableset.
+
+    Device-memory admission: the tables and every engine's buffers count
+    against `budget` bytes. Engine buffers only grow (ngap_engine_memory), so
+    a batch is launched on a slot only when what it would add to that
+    engine (a larger input copy, a larger unit plan) keeps the total within
+    the budget. Each engine's fixed part (report buffers for `rep_cap`
+    reports, per-warp overflow stacks) is allocated by a one-stream warm-up
+    batch at construction, so it is counted from the start; a budget that
+    cannot hold the tables and those parts raises ValueError. A request that
+    can never be admitted (longer than max_batch_bytes, or needing more than
+    the budget leaves with every engine as it is) is rejected at arrival:
+    its `error` is set and it gets no reports.
+    """
+
+    UNIT_BYTES = 80  # device bytes of a unit record plus its share of a task record
+
+    def __init__(self, tableset, predictor=None, rho_ref=2.0, slots=2, budget=1 << 30,
+                 max_batch_bytes=64 << 20, device=0, queue_capacity=0,
+                 algorithm="nonblockingpcgroups", base_chunk=2048, chunk_lo=256, chunk_hi=2048,
+                 slot_factory=None, tables_bytes=None, isolate=False, heavy_work=None,
+                 adapt_chunks=True):
+        self.ts = tableset
+        self.pred = predictor
+        self.isolate = bool(isolate and predictor is not None and len(range(slots)) > 1)
+        self.heavy_work = heavy_work
+        self.adapt_chunks = adapt_chunks
+        self.rho_ref = rho_ref
+        self.base_chunk = base_chunk
+        self.chunk_lo, self.chunk_hi = chunk_lo, chunk_hi
+        self.budget = budget
+        self.max_bytes = max_batch_bytes
+        self.queue_capacity = queue_capacity
+        self.algorithm = algorithm
+        self.rep_cap = max(1 << 16, max_batch_bytes // 4)
+        if tables_bytes is None:
+            tables_bytes = sum(t.device_bytes for t in getattr(tableset, "tables", []))
+        self.tables_bytes = int(tables_bytes)
+        self.max_tiles = max([t.stats()["tiles"] for t in getattr(tableset, "tables", [])] or [1])
+        make = slot_factory or (lambda i: EngineSlot(tableset, device, max_batch_bytes))
+        self.slots = [make(i) for i in range(slots)]
+        self.busy = [None] * slots      # (batch, launch time)
+        self.batches = []               # (size, bytes, predicted work, device ms)
+        self.launches = 0               # kernels launched by the served batches
+        self.rejected = []              # requests that can never be admitted
+        for sl in self.slots:           # allocate each engine's fixed part now
+            sl.launch([Request(-1, 0, np.zeros(16, np.uint8), 0.0)], self._params())
+            sl.finish(1)
+        self.mem = [sl.memory() for sl in self.slots]
+        if self.tables_bytes + sum(self._held(m) for m in self.mem) > budget:
+            raise ValueError(f"a budget of {budget} bytes does not hold the tables "
+                             f"({self.tables_bytes}) and the engines' fixed buffers "
+                             f"({sum(self._held(m) for m in self.mem)})")
+
+    def _params(self):
+        return dict(algorithm=self.algorithm, result_capacity=self.rep_cap,
+                    queue_capacity=self.queue_capacity)
+
+    @staticmethod
+    def _held(m):
+        return m["input"] + m["reports"] + m["scratch"] + m["plan"]
+
+    def held_bytes(self):
+        """Device bytes held now: tables plus every engine's buffers."""
+        return self.tables_bytes + sum(self._held(m) for m in self.mem)
+
+    def _growth(self, s, nbytes, nreq):
+        """Bytes slot s's engine would add for a batch of nbytes in nreq streams:
+        a larger input copy, and room for a unit plan at the shortest chunk."""
+        m = self.mem[s]
+        plan = self.UNIT_BYTES * self.max_tiles * (nbytes // max(1, self.chunk_lo) + 2 * nreq)
+        return max(0, padded_input(nbytes) - m["input"]) + max(0, plan - m["plan"])
+
+    def _fits(self, s, nbytes, nreq):
+        return self.held_bytes() + self._growth(s, nbytes, nreq) <= self.budget
+
+    def admissible(self, r):
+        """Whether request r alone could ever be admitted (engines never shrink)."""
+        n = len(r.data)
+        return n <= self.max_bytes and any(self._fits(s, n, 1) for s in range(len(self.slots)))
+
+    def _form(self, queue, s):
+        """Requests for the next batch on slot s, in arrival order, while the
+        batch fits max_batch_bytes and the device-memory budget (removed from
         queue)."""
-        free = self.budget - self._held()
         n, nbytes = 0, 0
         while n < len(queue):
             nb = nbytes + len(queue[n].data)
-            if nb > self.max_bytes or self._reserve(nb) > free:
+            if nb > self.max_bytes or not self._fits(s, nb, n + 1):
                 break
             n, nbytes = n + 1, nb
         chosen = queue[:n]
         del queue[:n]
         return chosen
 
+    def _finish(self, s):
+        batch, _ = self.busy[s]
+        per, dev_ms, launches = self.slots[s].finish(len(batch))
+        self.launches += launches
+        self.mem[s] = self.slots[s].memory()
+        t = time.perf_counter() - self._t0
+        for r, rep in zip(batch, per):
+            r.reports = rep
+            r.done = t
+        self.batches.append((len(batch), sum(len(r.data) for r in batch),
+                             sum(r.pred_work for r in batch), dev_ms))
+        self.busy[s] = None
+
     def run(self, requests):
-        """Serves requests (sorted by arrival) in real time; returns metrics."""
+        """Serves requests (sorted by arrival) in real time; returns metrics.
+
+        Without isolation, batches take the queue in arrival order. With
+        isolation (a predictor and at least two slots), a request whose
+        predicted work (density x length) exceeds heavy_work goes to the heavy
+        queue: slot 0 serves only the light queue, the other slots the heavy
+        queue first and the light one when it is empty, so that light requests
+        never share a batch with (and wait for) a predicted-heavy one."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        queue, nxt = [], 0
+        light, heavy, nxt = [], [], 0
         self._t0 = time.perf_counter()
-        while nxt < len(reqs) or queue or any(b is not None for b in self.busy):
+        while nxt < len(reqs) or light or heavy or any(b is not None for b in self.busy):
             now = time.perf_counter() - self._t0
-            first = nxt
+            fresh = []
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                queue.append(reqs[nxt])
+                r = reqs[nxt]
                 nxt += 1
-            if self.pred is not None and nxt > first:  # predictions at arrival, inside the clock
-                rho = self.pred.density(reqs[first:nxt])
+                if self.admissible(r):
+                    fresh.append(r)
+                else:
+                    r.error = (f"request of {len(r.data)} bytes can never be admitted "
+                               f"(max_batch_bytes {self.max_bytes}, budget {self.budget})")
+                    r.done = now
+                    self.rejected.append(r)
+            if self.pred is not None and fresh:  # predictions at arrival, inside the clock
+                rho = self.pred.density(fresh)
                 chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk, self.chunk_lo,
                                       self.chunk_hi)
-                for r, d, c in zip(reqs[first:nxt], rho, chunks):
+                for r, d, c in zip(fresh, rho, chunks):
                     r.pred_work = float(d) * len(r.data)
-                    r.chunk = int(c)
+                    r.chunk = int(c) if self.adapt_chunks else 0
+            for r in fresh:
+                if self.isolate and self.heavy_work is not None and r.pred_work > self.heavy_work:
+                    heavy.append(r)
+                else:
+                    light.append(r)
             for s, b in enumerate(self.busy):
-                if b is not None and b[1].query():
-                    self._finish(s, now)
+                if b is not None and self.slots[s].done():
+                    self._finish(s)
             for s in range(len(self.busy)):
-                if self.busy[s] is None and queue:
-                    batch = self._form(queue)
+                if self.busy[s] is not None:
+                    continue
+                if not self.isolate:
+                    q = light if light else heavy
+                elif s == 0:
+                    q = light
+                else:
+                    q = heavy if heavy else light
+                if q:
+                    batch = self._form(q, s)
                     if batch:
-                        self._launch(s, batch)
-            if not queue and nxt < len(reqs) and all(b is None for b in self.busy):
+                        self.slots[s].launch(batch, self._params())
+                        self.mem[s] = self.slots[s].memory()
+                        self.busy[s] = (batch, now)
+            if not light and not heavy and nxt < len(reqs) and all(b is None for b in self.busy):
                 time.sleep(max(0.0, min(reqs[nxt].arrival - now, 0.0005)))
-        return summarize(reqs, self.batches)
+        return summarize([r for r in reqs if r.error is None], self.batches,
+                         rejected=len(self.rejected))
 
 
-def summarize(reqs, batches):
+def summarize(reqs, batches, rejected=0):
     lat = np.array([(r.done - r.arrival) * 1e3 for r in reqs])
     nbytes = sum(len(r.data) for r in reqs)
     span = max(r.done for r in reqs) - min(r.arrival for r in reqs) if reqs else 0.0
@@ -253,5 +363,5 @@ def summarize(reqs, batches):
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "mean_ms": float(lat.mean()) if len(lat) else None,
             "MBps": nbytes / span / 1e6 if span > 0 else None,
-            "batches": len(batches),
+            "batches": len(batches), "rejected": rejected,
             "mean_batch": float(np.mean([b[0] for b in batches])) if batches else 0.0}

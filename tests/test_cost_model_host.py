@@ -79,24 +79,84 @@ def test_autotune_sample_streams():
     assert len(at.sample_streams(lengths, frac=1.0)) == 200
 
 
-def _server(budget, max_bytes, held=()):
-    s = sv.Server.__new__(sv.Server)  # the admission rule only: no engines or streams
-    s.budget, s.max_bytes = budget, max_bytes
-    s.busy = [(None, None, h, None) for h in held] + [None]
-    return s
+class FakeSlot:
+    """A serving slot without a GPU: memory grows like an engine's (input copy
+    to the largest batch, fixed report and scratch parts from the warm-up
+    batch) and a batch completes after `polls` done() queries."""
+
+    def __init__(self, fixed=1000, polls=2):
+        self.fixed, self.polls = fixed, polls
+        self.mem = {"input": 0, "reports": 0, "scratch": 0, "plan": 0}
+        self.launched = []
+        self.left = 0
+
+    def memory(self):
+        return dict(self.mem)
+
+    def launch(self, batch, params):
+        n = sum(len(r.data) for r in batch)
+        self.mem["input"] = max(self.mem["input"], sv.padded_input(n))
+        self.mem["reports"] = self.mem["scratch"] = self.fixed // 2
+        self.launched.append([r.rid for r in batch])
+        self.left = self.polls
+
+    def done(self):
+        self.left -= 1
+        return self.left <= 0
+
+    def finish(self, nreq):
+        return [np.array([rid], np.int64) for rid in self.launched[-1]], 0.5, 3
 
 
-def test_serving_admission():
-    reqs = [sv.Request(i, 0, np.zeros(n, np.uint8), 0.0) for i, n in enumerate([40, 30, 20, 50])]
-    q = list(reqs)
-    s = _server(budget=1000, max_bytes=90)  # batch capped by max_batch_bytes, in arrival order
-    assert [r.rid for r in s._form(q)] == [0, 1, 2] and [r.rid for r in q] == [3]
-    q = list(reqs)
-    s = _server(budget=100, max_bytes=1000, held=(35,))  # 65 bytes free under the budget
-    assert [r.rid for r in s._form(q)] == [0] and len(q) == 3
-    q = list(reqs)
-    s = _server(budget=100, max_bytes=1000, held=(80,))  # the first request does not fit: none
-    assert s._form(q) == [] and len(q) == 4
+def _server(budget, max_bytes, slots=1, fixed=1000, tables=100):
+    made = []
+
+    def factory(i):
+        made.append(FakeSlot(fixed))
+        return made[-1]
+    srv = sv.Server(None, slots=slots, budget=budget, max_batch_bytes=max_bytes, chunk_lo=1 << 30,
+                    slot_factory=factory, tables_bytes=tables)
+    return srv, made
+
+
+def _reqs(sizes):
+    return [sv.Request(i, 0, np.zeros(n, np.uint8), 0.0) for i, n in enumerate(sizes)]
+
+
+def test_serving_admission_counts_engine_buffers():
+    # tables 100 + fixed 1000 + the warm-up batch's input copy (16 B -> 80)
+    srv, made = _server(budget=10_000, max_bytes=1000)
+    assert srv.held_bytes() == 100 + 1000 + 80
+    q = _reqs([400, 300, 200, 500])  # capped by max_batch_bytes, in arrival order
+    assert [r.rid for r in srv._form(q, 0)] == [0, 1, 2] and [r.rid for r in q] == [3]
+    # held 1180; a batch adds its padded input beyond the 80 held and a unit
+    # plan of 80 B x (2 per stream): 400 B -> 384 + 160 = 544 (1724 <= 1800),
+    # 700 B in two streams -> 704 + 320 = 1024 (2204 > 1800)
+    srv, made = _server(budget=1800, max_bytes=10_000)
+    q = _reqs([400, 300, 200])
+    got = srv._form(q, 0)
+    assert [r.rid for r in got] == [0] and len(q) == 2
+    with pytest.raises(ValueError):  # the fixed parts alone exceed the budget
+        _server(budget=1000, max_bytes=1000)
+
+
+def test_serving_rejects_requests_that_never_fit():
+    # held 100 + 2 x 1080 = 2260; a lone request of n bytes adds (pad(n) - 80) + 160:
+    # 900 -> 1064 (3324 > 3000), 300 -> 444 (2704), 200 -> 352, 100 -> 256
+    srv, made = _server(budget=3000, max_bytes=1000, slots=2)
+    reqs = _reqs([300, 5000, 200, 900, 100])  # 5000 > max_batch_bytes; 900 > the budget
+    m = srv.run(reqs)  # returns instead of waiting forever
+    assert m["rejected"] == 2 and m["requests"] == 3
+    bad = {r.rid for r in reqs if r.error}
+    assert bad == {1, 3} and all("never be admitted" in reqs[i].error for i in bad)
+    served = sorted(rid for s in made for b in s.launched for rid in b if rid >= 0)
+    assert served == [0, 2, 4]
+    for r in reqs:
+        if r.error is None:
+            assert r.reports is not None and int(r.reports[0]) == r.rid and r.done >= r.arrival
+        else:
+            assert r.reports is None
+    assert srv.held_bytes() <= srv.budget
 
 
 def test_autotune_search_with_fake_launches():
@@ -133,3 +193,39 @@ def test_autotune_search_with_fake_launches():
     assert len(calls) == 8 * 3 + 4
     with pytest.raises(ValueError):
         at.autotune(None, None, data, offsets, lengths, nfa_of, tile_grid=[{}], run=run)
+
+
+class FakePredictor:
+    """Density per request from a table (rid -> entries per byte)."""
+
+    def __init__(self, dens):
+        self.dens = dens
+
+    def density(self, reqs):
+        return np.array([self.dens[r.rid] for r in reqs], np.float64)
+
+
+def test_serving_isolation_keeps_heavy_requests_apart():
+    """With isolation, requests predicted heavier than heavy_work never share a
+    batch with light ones; slot 0 serves only light requests."""
+    made = []
+
+    def factory(i):
+        made.append(FakeSlot(1000, polls=3))
+        return made[-1]
+    sizes = [100] * 12
+    heavy_ids = {2, 5, 9}
+    dens = {i: (50.0 if i in heavy_ids else 1.0) for i in range(12)}
+    srv = sv.Server(None, predictor=FakePredictor(dens), slots=2, budget=1 << 30,
+                    max_batch_bytes=10_000, chunk_lo=1 << 30, slot_factory=factory,
+                    tables_bytes=0, isolate=True, heavy_work=1000.0, adapt_chunks=False)
+    reqs = [sv.Request(i, 0, np.zeros(n, np.uint8), 0.0) for i, n in enumerate(sizes)]
+    m = srv.run(reqs)
+    assert m["requests"] == 12 and m["rejected"] == 0
+    batches = [b for s in made for b in s.launched if -1 not in b]
+    for b in batches:
+        kinds = {rid in heavy_ids for rid in b}
+        assert len(kinds) == 1, b  # never mixed
+    assert all(not (set(b) & heavy_ids) for b in made[0].launched if -1 not in b)
+    assert all(r.reports is not None and int(r.reports[0]) == r.rid for r in reqs)
+    assert all(r.chunk == 0 for r in reqs)  # fixed chunks when adapt_chunks is off
