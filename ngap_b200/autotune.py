@@ -3,8 +3,8 @@
 The reference tunes by brute force over fetch size, active threshold and AAS
 interval, rerunning the whole input for each point (code/src/ngap/ngap.cu:
 1995-2056). Here the knobs are the engine's own: worklist window, chunk
-length of acyclic tiles and algorithm variant (with or without
-privatization) by default; queue capacity (`queue_capacity` in the grid: a
+length of acyclic tiles, algorithm variant (with or without
+privatization) and CUDA-graph replay of the whole step by default; queue capacity (`queue_capacity` in the grid: a
 candidate whose overflow stacks run out on the sample is skipped) and the
 tile partition (`tile_grid`: table options per candidate, one tableset built
 for each) on request. Each candidate runs on a sample of the streams (a few
@@ -22,6 +22,7 @@ DEFAULT_GRID = {
     "window": [512, 1024, 2048],
     "chunk": [0, 4096, 16384],
     "algorithm": ["nonblockingpcgroups", "nonblockingallgroups"],
+    "use_graph": [False, True],
 }
 
 
@@ -78,6 +79,9 @@ def autotune(engine, tableset, data, offsets, lengths, nfa_of, grid=None, frac=0
     buf = np.concatenate([data[offsets[i]:offsets[i] + lengths[i]] for i in idx]) \
         if len(idx) else np.zeros(0, np.uint8)
     nf = np.asarray(nfa_of)[idx]
+    if run is _run_on_device:  # the sample on the device: a captured graph replays its copy
+        import torch
+        buf = torch.from_numpy(buf).to(f"cuda:{engine.device}")
     tilesets = [(None, tableset)]
     if tile_grid:
         tilesets = [(dict(opts), make_tableset(dict(opts))) for opts in tile_grid]
