@@ -54,7 +54,7 @@ __host__ __device__ inline uint32_t prefix_hash(uint32_t key) {
 // (one class word) follow each state's 4 x u32 with its successors' class
 // masks (4 x u32, 0 for none), a 32-byte record. cmask: bit c of
 // word c/32 = the state accepts byte class c. cls: byte -> class id, live
-// classes first (identity when cw == 8).
+// classes first, the dead class (bytes no state accepts) last.
 struct TileDev {
   int32_t group = 0;        // group of the first CC (report ids are in sid)
   int32_t nstates = 0;

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cstring>
 #include <map>
+#include <functional>
 #include <mutex>
 #include <memory>
 #include <tuple>
@@ -77,6 +78,7 @@ struct ngap_tables {
   int32_t image_region = 0;  // shared-memory bytes reserved for tile images
   std::vector<int32_t> pair_nact;  // activation slots of each (activation, layered) tile pair
   int32_t max_nact = 0;            // largest pair
+  bool lean = true;                // no tile has sticky states or an activation/layered pass
 
   ~ngap_tables() {
     for (void* p : allocs) cudaFree(p);
@@ -123,6 +125,8 @@ struct ngap_engine {
   size_t tasks_cap = 0;
   int32_t ntasks = 0;
   int32_t ntasks1 = 0;       // tasks of activation tiles, launched first
+  int32_t free_range[4] = {0, 0, 0, 0};  // free units: [begin, count) of each launch
+  int32_t free_tile[2] = {-1, -1};       // the one tile of each launch's free units, or -1
   // worklist traces
   bool trace = false;
   unsigned long long* d_unit_work = nullptr;
@@ -248,6 +252,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       return NGAP_E_UNSUPPORTED;
     }
     t->max_states = std::max(t->max_states, th.nstates);
+    t->lean = t->lean && th.nsticky == 0 && th.phase == 0;
     TileDev d;
     d.group = th.group;
     d.nstates = th.nstates;
@@ -333,7 +338,7 @@ int ngap_engine_create(int device, ngap_engine** out) {
   CUDA_TRY(cudaFuncSetAttribute(small_sort_unique<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSmallSortSmem));
   CUDA_TRY(cudaMalloc(&e->d_err, sizeof(int)));
-  CUDA_TRY(cudaMalloc(&e->d_unit_counter, sizeof(unsigned int)));
+  CUDA_TRY(cudaMalloc(&e->d_unit_counter, 2 * sizeof(unsigned int)));  // tasks, free units
   CUDA_TRY(cudaMallocHost(&e->h_counters, kNumCounters * sizeof(unsigned long long)));
   for (auto& ev : e->ev) CUDA_TRY(cudaEventCreate(&ev));
   *out = e.release();
@@ -350,6 +355,14 @@ void ngap_engine_destroy(ngap_engine* e) {
 }  // extern "C"
 
 namespace {
+
+// New capacity of a grow-only buffer that must hold `need` elements: at
+// least twice the old one, so that a run of growing plans reallocates (a
+// cudaMalloc, which waits for the device) only a few times.
+template <class T>
+T grown(T cap, T need) {
+  return std::max(need, cap * 2);
+}
 
 int ensure_reports(ngap_engine* e, uint64_t cap) {
   if (cap <= e->rep_cap) return NGAP_OK;
@@ -490,19 +503,41 @@ struct ActRows {
   }
 };
 
-// Units (already grouped by tile) -> CTA tasks: the long units of cyclic tiles
-// first, one per warp of a task; chunks after them in tasks sized to give
-// every CTA several tasks.
+// Units (already grouped by tile) -> work of the launches. Units of tiles
+// whose image is staged in shared memory become CTA tasks: the long units of
+// cyclic tiles first, one per warp of a task; chunks after them in tasks sized
+// to give every CTA several tasks. Units of tiles read in place (is_free)
+// are taken one by one by warps (free units), after the tasks of their
+// launch. Layout of `units`: [activation tasks][activation free]
+// [cyclic tasks][chunk tasks][cyclic free][chunk free]; free_range holds
+// (begin, count) of the free units of the first and of the second launch.
 void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
                 const std::vector<UnitDev>& unbounded, const std::vector<UnitDev>& bounded,
-                int grid, std::vector<TaskDev>& tasks, int32_t* ntasks1) {
+                int grid, const std::function<bool(int)>& is_free, std::vector<TaskDev>& tasks,
+                int32_t* ntasks1, int32_t free_range[4], int32_t free_tile[2]) {
   units.clear();
   tasks.clear();
-  units.insert(units.end(), pass1.begin(), pass1.end());
-  const size_t np1 = units.size();
-  units.insert(units.end(), unbounded.begin(), unbounded.end());
-  const size_t nunb = units.size();
-  units.insert(units.end(), bounded.begin(), bounded.end());
+  auto split = [&](const std::vector<UnitDev>& src, std::vector<UnitDev>& st,
+                   std::vector<UnitDev>& fr) {
+    for (const UnitDev& u : src) (is_free(u.tile) ? fr : st).push_back(u);
+  };
+  std::vector<UnitDev> p1s, p1f, ubs, ubf, bs, bf;
+  split(pass1, p1s, p1f);
+  split(unbounded, ubs, ubf);
+  split(bounded, bs, bf);
+  // a launch whose free units all belong to one tile: its CTAs stage that
+  // tile's descriptors in shared memory once
+  auto one_tile = [](const std::vector<UnitDev>& a, const std::vector<UnitDev>& b) {
+    int tile = -1;
+    for (const auto* v : {&a, &b})
+      for (const UnitDev& u : *v) {
+        if (tile >= 0 && u.tile != tile) return -1;
+        tile = u.tile;
+      }
+    return tile;
+  };
+  free_tile[0] = one_tile(p1f, {});
+  free_tile[1] = one_tile(ubf, bf);
   auto per = [&](size_t n) {
     return std::max<int64_t>(kWarpsPerCta,
                              std::min<int64_t>(512, (int64_t)n / std::max(1, 4 * grid)));
@@ -532,14 +567,28 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
       i = j;
     }
   };
-  cut(0, np1, per(pass1.size()));
+  auto append = [&](const std::vector<UnitDev>& v) {
+    const size_t b = units.size();
+    units.insert(units.end(), v.begin(), v.end());
+    return b;
+  };
+  size_t b = append(p1s);
+  cut(b, units.size(), per(p1s.size()));
   *ntasks1 = (int32_t)tasks.size();
-  cut(np1, nunb, kWarpsPerCta);
-  cut(nunb, units.size(), per(bounded.size()));
+  free_range[0] = (int32_t)append(p1f);
+  free_range[1] = (int32_t)p1f.size();
+  b = append(ubs);
+  cut(b, units.size(), kWarpsPerCta);
+  b = append(bs);
+  cut(b, units.size(), per(bs.size()));
+  free_range[2] = (int32_t)append(ubf);
+  append(bf);
+  free_range[3] = (int32_t)(ubf.size() + bf.size());
 }
 
 ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
-                   std::vector<UnitDev>& units, std::vector<TaskDev>& tasks, int32_t* ntasks1) {
+                   std::vector<UnitDev>& units, std::vector<TaskDev>& tasks, int32_t* ntasks1,
+                   int32_t free_range[4], int32_t free_tile[2]) {
   std::vector<UnitDev> pass1, unbounded, bounded;
   ActRows rows({t}, k.num_seg);
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
@@ -550,7 +599,10 @@ ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
                 unbounded, bounded);
     }
   }
-  make_tasks(units, pass1, unbounded, bounded, grid, tasks, ntasks1);
+  const int32_t region = t->image_region;
+  auto is_free = [&](int tile) { return (int32_t)t->tiles[tile].image.size() > region; };
+  make_tasks(units, pass1, unbounded, bounded, grid, is_free, tasks, ntasks1, free_range,
+             free_tile);
   return rows;
 }
 
@@ -559,11 +611,12 @@ int trace_buffer(ngap_engine* e, cudaStream_t st, unsigned long long** out) {
   *out = nullptr;
   if (!e->trace || e->nunits == 0) return NGAP_OK;
   if ((size_t)e->nunits > e->unit_work_cap) {
+    const size_t cap = grown(e->unit_work_cap, (size_t)e->nunits);
     cudaFree(e->d_unit_work);
     e->d_unit_work = nullptr;
     e->unit_work_cap = 0;
-    CUDA_TRY(cudaMalloc(&e->d_unit_work, (size_t)e->nunits * sizeof(unsigned long long)));
-    e->unit_work_cap = (size_t)e->nunits;
+    CUDA_TRY(cudaMalloc(&e->d_unit_work, cap * sizeof(unsigned long long)));
+    e->unit_work_cap = cap;
   }
   CUDA_TRY(cudaMemsetAsync(e->d_unit_work, 0, (size_t)e->nunits * sizeof(unsigned long long), st));
   *out = e->d_unit_work;
@@ -575,15 +628,17 @@ int set_act_rows(ngap_engine* e, const ActRows& rows) {
   e->act_entries = rows.total;
   e->act_rows = (int32_t)rows.row_off.size();
   if (e->act_entries > e->act_cap) {
+    const int64_t cap = grown(e->act_cap, e->act_entries);
     cudaFree(e->d_act);
     cudaFree(e->d_act_list);
     e->d_act = e->d_act_list = nullptr;
     e->act_cap = 0;
-    CUDA_TRY(cudaMalloc(&e->d_act, (size_t)e->act_entries * sizeof(uint32_t)));
-    CUDA_TRY(cudaMalloc(&e->d_act_list, (size_t)e->act_entries * sizeof(uint32_t)));
-    e->act_cap = e->act_entries;
+    CUDA_TRY(cudaMalloc(&e->d_act, (size_t)cap * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&e->d_act_list, (size_t)cap * sizeof(uint32_t)));
+    e->act_cap = cap;
   }
   if (e->act_rows > e->rows_cap) {
+    const int32_t cap = grown(e->rows_cap, e->act_rows);
     cudaFree(e->d_row_off);
     cudaFree(e->d_row_n);
     cudaFree(e->d_act_cnt);
@@ -591,10 +646,10 @@ int set_act_rows(ngap_engine* e, const ActRows& rows) {
     e->d_row_n = nullptr;
     e->d_act_cnt = nullptr;
     e->rows_cap = 0;
-    CUDA_TRY(cudaMalloc(&e->d_row_off, (size_t)e->act_rows * sizeof(int64_t)));
-    CUDA_TRY(cudaMalloc(&e->d_row_n, (size_t)e->act_rows * sizeof(int32_t)));
-    CUDA_TRY(cudaMalloc(&e->d_act_cnt, (size_t)e->act_rows * sizeof(uint32_t)));
-    e->rows_cap = e->act_rows;
+    CUDA_TRY(cudaMalloc(&e->d_row_off, (size_t)cap * sizeof(int64_t)));
+    CUDA_TRY(cudaMalloc(&e->d_row_n, (size_t)cap * sizeof(int32_t)));
+    CUDA_TRY(cudaMalloc(&e->d_act_cnt, (size_t)cap * sizeof(uint32_t)));
+    e->rows_cap = cap;
   }
   if (e->act_rows > 0) {
     CUDA_TRY(cudaMemcpy(e->d_row_off, rows.row_off.data(), rows.row_off.size() * sizeof(int64_t),
@@ -627,16 +682,37 @@ __global__ void act_compact(const int64_t* __restrict__ row_off, const int32_t* 
 
 // The matching launches of a plan: the activation tiles' tasks, then the rest
 // (the layered tiles read what the first launch recorded).
-template <int PRIV>
+// CTAs one launch needs: one per task, plus one per kWarpsPerCta free units,
+// at most the grid.
+int launch_grid(const ngap_engine* e, int ntasks, int nfree) {
+  const int64_t want = (int64_t)ntasks + ((int64_t)nfree + kWarpsPerCta - 1) / kWarpsPerCta;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(e->grid, want));
+}
+
+int plan_grid(const ngap_engine* e, int full_grid) {
+  const int64_t want = (int64_t)e->ntasks +
+                       ((int64_t)e->free_range[1] + e->free_range[3] + kWarpsPerCta - 1) / kWarpsPerCta;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(full_grid, want));
+}
+
+// The matching launches of a plan: the activation tiles' work, then the rest
+// (the layered tiles read what the first launch recorded). Each launch takes
+// its tasks first, then its free units.
+template <int PRIV, bool LEAN>
 int launch_plan(ngap_engine* e, MatchParams mp, int smem, cudaStream_t st) {
+  unsigned int* free_cursor = e->d_unit_counter + 1;
+  mp.free_cursor = free_cursor;
   if (e->act_entries > 0)
     CUDA_TRY(cudaMemsetAsync(e->d_act, 0xff, (size_t)e->act_entries * sizeof(uint32_t), st));
-  if (e->ntasks1 > 0) {
+  if (e->ntasks1 > 0 || e->free_range[1] > 0) {
     mp.ntasks = e->ntasks1;
-    match_kernel<PRIV><<<std::max(1, std::min(e->grid, e->ntasks1)), kCtaThreads, smem, st>>>(mp);
+    mp.free_begin = e->free_range[0];
+    mp.nfree = e->free_range[1];
+    mp.free_tile = e->free_tile[0];
+    CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, 2 * sizeof(unsigned int), st));
+    match_kernel<PRIV, LEAN><<<launch_grid(e, mp.ntasks, mp.nfree), kCtaThreads, smem, st>>>(mp);
     CUDA_TRY(cudaGetLastError());
     e->launches++;
-    CUDA_TRY(cudaMemsetAsync(mp.task_counter, 0, sizeof(unsigned int), st));
   }
   if (e->act_rows > 0) {
     act_compact<<<(e->act_rows + 7) / 8, 256, 0, st>>>(e->d_row_off, e->d_row_n, e->act_rows,
@@ -644,14 +720,29 @@ int launch_plan(ngap_engine* e, MatchParams mp, int smem, cudaStream_t st) {
     CUDA_TRY(cudaGetLastError());
     e->launches++;
   }
-  if (e->ntasks > e->ntasks1) {
+  if (e->ntasks > e->ntasks1 || e->free_range[3] > 0) {
     mp.tasks = e->d_tasks + e->ntasks1;
     mp.ntasks = e->ntasks - e->ntasks1;
-    match_kernel<PRIV><<<std::max(1, std::min(e->grid, mp.ntasks)), kCtaThreads, smem, st>>>(mp);
+    mp.free_begin = e->free_range[2];
+    mp.nfree = e->free_range[3];
+    mp.free_tile = e->free_tile[1];
+    CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, 2 * sizeof(unsigned int), st));
+    match_kernel<PRIV, LEAN><<<launch_grid(e, mp.ntasks, mp.nfree), kCtaThreads, smem, st>>>(mp);
     CUDA_TRY(cudaGetLastError());
     e->launches++;
   }
   return NGAP_OK;
+}
+
+int launch_any(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t st, int priv,
+               bool lean) {
+  if (lean)
+    return priv == 0 ? launch_plan<0, true>(e, mp, smem, st)
+                     : priv == 1 ? launch_plan<1, true>(e, mp, smem, st)
+                                 : launch_plan<2, true>(e, mp, smem, st);
+  return priv == 0 ? launch_plan<0, false>(e, mp, smem, st)
+                   : priv == 1 ? launch_plan<1, false>(e, mp, smem, st)
+                               : launch_plan<2, false>(e, mp, smem, st);
 }
 
 __global__ void swap_halves(uint64_t* a, uint64_t n) {
@@ -675,11 +766,12 @@ int set_smem(ngap_engine* e, int smem) {
     e->max_smem_set = g_smem_set[dev];
     return NGAP_OK;
   }
-  cudaError_t ce = cudaFuncSetAttribute(match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (ce == cudaSuccess)
-    ce = cudaFuncSetAttribute(match_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (ce == cudaSuccess)
-    ce = cudaFuncSetAttribute(match_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const void* kernels[6] = {(const void*)match_kernel<0, false>, (const void*)match_kernel<1, false>,
+                            (const void*)match_kernel<2, false>, (const void*)match_kernel<0, true>,
+                            (const void*)match_kernel<1, true>, (const void*)match_kernel<2, true>};
+  cudaError_t ce = cudaSuccess;
+  for (int k = 0; k < 6 && ce == cudaSuccess; k++)
+    ce = cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (ce != cudaSuccess) {
     set_error("shared memory request of %d bytes rejected: %s", smem, cudaGetErrorString(ce));
     return NGAP_E_CUDA;
@@ -691,7 +783,8 @@ int set_smem(ngap_engine* e, int smem) {
 
 template <int PRIV>
 int blocks_per_sm(int smem, int* out) {
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, match_kernel<PRIV>, kCtaThreads, smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, match_kernel<PRIV, false>, kCtaThreads,
+                                                         smem));
   if (*out < 1) {
     set_error("the matching kernel does not fit on an SM with %d bytes of shared memory", smem);
     return NGAP_E_CUDA;
@@ -979,22 +1072,25 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     std::vector<UnitDev> units;
     std::vector<TaskDev> tasks;
     int32_t ntasks1 = 0;
-    const ActRows rows = plan_units(t, key, full_grid, units, tasks, &ntasks1);
+    const ActRows rows = plan_units(t, key, full_grid, units, tasks, &ntasks1, e->free_range,
+                                    e->free_tile);
     e->ntasks1 = ntasks1;
     if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
+      const size_t cap = grown(e->units_cap, units.size());
       cudaFree(e->d_units);
       e->d_units = nullptr;
       e->units_cap = 0;
-      CUDA_TRY(cudaMalloc(&e->d_units, units.size() * sizeof(UnitDev)));
-      e->units_cap = units.size();
+      CUDA_TRY(cudaMalloc(&e->d_units, cap * sizeof(UnitDev)));
+      e->units_cap = cap;
     }
     if (tasks.size() > e->tasks_cap) {
+      const size_t cap = grown(e->tasks_cap, tasks.size());
       cudaFree(e->d_tasks);
       e->d_tasks = nullptr;
       e->tasks_cap = 0;
-      CUDA_TRY(cudaMalloc(&e->d_tasks, tasks.size() * sizeof(TaskDev)));
-      e->tasks_cap = tasks.size();
+      CUDA_TRY(cudaMalloc(&e->d_tasks, cap * sizeof(TaskDev)));
+      e->tasks_cap = cap;
     }
     if (!units.empty())
       CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
@@ -1009,9 +1105,11 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     e->plan_key = key;
     e->batch_ts = 0;  // the batched plan cache no longer describes the buffers
   }
-  const int grid = std::max(1, std::min(full_grid, e->ntasks));
+  const int grid = plan_grid(e, full_grid);
   e->grid = grid;
-  rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, t->max_states, t->max_nact, kDefaultQueue);
+  // per-warp scratch for the full grid, whatever this plan uses: a later
+  // larger plan then never reallocates (cudaMalloc waits for the device)
+  rc = ensure_slots(e, (size_t)full_grid * kWarpsPerCta, t->max_states, t->max_nact, kDefaultQueue);
   if (rc != NGAP_OK) return rc;
 
   CUDA_TRY(cudaEventRecord(e->ev[0], st));
@@ -1021,7 +1119,6 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
     CUDA_TRY(cudaMemcpyAsync(e->d_input, input, total, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemsetAsync(e->d_counters, 0, 8 * sizeof(unsigned long long), st));
   CUDA_TRY(cudaMemsetAsync(e->d_err, 0, sizeof(int), st));
-  CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, sizeof(unsigned int), st));
 
   MatchParams mp;
   mp.tiles = t->d_tiles;
@@ -1060,10 +1157,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   if ((rc = trace_buffer(e, st, &mp.unit_work)) != NGAP_OK) return rc;
   e->trace_seg_len = p->seg_len;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
-  if (e->ntasks > 0) {
-    if (priv == 0) rc = launch_plan<0>(e, mp, smem, st);
-    else if (priv == 1) rc = launch_plan<1>(e, mp, smem, st);
-    else rc = launch_plan<2>(e, mp, smem, st);
+  if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0) {
+    rc = launch_any(e, mp, smem, st, priv, t->lean);
     if (rc != NGAP_OK) return rc;
   }
   CUDA_TRY(cudaEventRecord(e->ev[2], st));
@@ -1295,6 +1390,8 @@ struct ngap_tableset {
   TileDev* d_tiles = nullptr;
   int ntiles = 0, image_region = 0, max_states = 0, max_groups = 1, max_depth = 1, device = 0;
   int max_nact = 0;
+  std::vector<int32_t> image_bytes;  // per tile of the combined array
+  bool lean = true;                  // every table lean (see ngap_tables)
   ~ngap_tableset() { cudaFree(d_tiles); }
 };
 
@@ -1317,6 +1414,8 @@ int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset*
     ts->tables.push_back(t);
     ts->tile_base.push_back((int)all.size());
     all.insert(all.end(), t->dev_desc.begin(), t->dev_desc.end());
+    for (const TileDev& d : t->dev_desc) ts->image_bytes.push_back(d.image_bytes);
+    ts->lean = ts->lean && t->lean;
     ts->image_region = std::max(ts->image_region, t->image_region);
     ts->max_states = std::max(ts->max_states, t->max_states);
     ts->max_groups = std::max(ts->max_groups, t->num_groups);
@@ -1432,21 +1531,26 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
                     unbounded, bounded);
         }
     }
-    make_tasks(units, pass1, unbounded, bounded, full_grid, tasks, &e->ntasks1);
+    const int32_t region = ts->image_region;
+    auto is_free = [&](int tile) { return ts->image_bytes[tile] > region; };
+    make_tasks(units, pass1, unbounded, bounded, full_grid, is_free, tasks, &e->ntasks1,
+               e->free_range, e->free_tile);
     if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
+      const size_t cap = grown(e->units_cap, units.size());
       cudaFree(e->d_units);
       e->d_units = nullptr;
       e->units_cap = 0;
-      CUDA_TRY(cudaMalloc(&e->d_units, units.size() * sizeof(UnitDev)));
-      e->units_cap = units.size();
+      CUDA_TRY(cudaMalloc(&e->d_units, cap * sizeof(UnitDev)));
+      e->units_cap = cap;
     }
     if (tasks.size() > e->tasks_cap) {
+      const size_t cap = grown(e->tasks_cap, tasks.size());
       cudaFree(e->d_tasks);
       e->d_tasks = nullptr;
       e->tasks_cap = 0;
-      CUDA_TRY(cudaMalloc(&e->d_tasks, tasks.size() * sizeof(TaskDev)));
-      e->tasks_cap = tasks.size();
+      CUDA_TRY(cudaMalloc(&e->d_tasks, cap * sizeof(TaskDev)));
+      e->tasks_cap = cap;
     }
     if (!units.empty())
       CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
@@ -1465,9 +1569,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     e->batch_chunk = p->chunk;
     replanned = true;
   }
-  const int grid = std::max(1, std::min(full_grid, e->ntasks));
+  const int grid = plan_grid(e, full_grid);
   e->grid = grid;
-  if ((rc = ensure_slots(e, (size_t)grid * kWarpsPerCta, ts->max_states, ts->max_nact,
+  if ((rc = ensure_slots(e, (size_t)full_grid * kWarpsPerCta, ts->max_states, ts->max_nact,
                          p->queue_capacity > 0 ? std::max(p->queue_capacity, 1024) : kDefaultQueue)) != NGAP_OK)
     return rc;
 
@@ -1517,11 +1621,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
       CUDA_TRY(cudaMemcpyAsync(e->d_input, input, input_bytes, cudaMemcpyHostToDevice, qs));
     CUDA_TRY(cudaMemsetAsync(e->d_counters, 0, 8 * sizeof(unsigned long long), qs));
     CUDA_TRY(cudaMemsetAsync(e->d_err, 0, sizeof(int), qs));
-    CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, sizeof(unsigned int), qs));
     int r = NGAP_OK;
-    if (e->ntasks > 0) {
-      r = priv == 0 ? launch_plan<0>(e, mp, smem, qs)
-                    : priv == 1 ? launch_plan<1>(e, mp, smem, qs) : launch_plan<2>(e, mp, smem, qs);
+    if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0) {
+      r = launch_any(e, mp, smem, qs, priv, ts->lean);
       if (r != NGAP_OK) return r;
     }
     if (!p->report_off) {

@@ -83,6 +83,10 @@ struct MatchParams {
   uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
   int32_t stk_g_cap;        // kStickyCap
   unsigned long long* unit_work;  // [units]: entries expanded + injected per unit (tracing), or null
+  int32_t free_begin;       // units [free_begin, free_begin + nfree) are taken warp by warp
+  int32_t nfree;
+  int32_t free_tile;        // the one tile of all free units (descriptors staged per CTA), or -1
+  unsigned int* free_cursor;  // next free unit (zeroed before the launch)
   int32_t wait_rounds;      // try_wait rounds before an mbarrier wait gives up
   int32_t skip_copy_unit;   // test hook: this unit's first window copy is not issued (-1: none),
                             // so its wait runs out and the launch reports kErrTimeout
@@ -140,7 +144,6 @@ struct WarpRun {
 // when the image does not fit) and the cold ones in global memory.
 struct TileView {
   const uint4* succ;    // wide tiles
-  const uint2* succ2;   // narrow tiles: 4 x u16
   const uint32_t* cmask;
   const uint32_t* rep;
   const uint32_t* sticky;  // sticky-state bitmap, nullptr when the tile has none
@@ -157,7 +160,7 @@ struct TileView {
 // Successors of v in the 32-bit convention (bit 31 = report, kNoSucc = none).
 __device__ __forceinline__ uint4 load_succ(const TileView& tv, uint32_t v) {
   if (!tv.narrow) return tv.succ[(size_t)v << tv.fused];
-  const uint2 x = tv.succ2[v];
+  const uint2 x = reinterpret_cast<const uint2*>(tv.succ)[v];  // narrow tiles: 4 x u16
   auto wide = [](uint32_t h) {
     return h == 0xffffu ? kNoSucc : ((h & 0x7fffu) | ((h & 0x8000u) << 16));
   };
@@ -1112,7 +1115,57 @@ __device__ __forceinline__ void expand_step2(const MatchParams& p, WarpSmem& ws,
   __syncwarp();
 }
 
-template <int PRIV>
+// A warp's view of one tile and the knobs derived from it.
+struct TileRun {
+  TileView tv;
+  int depth, batch, defer;
+  bool layered, wide_inject;
+};
+
+// Builds the view of tile t whose image is at ib (shared-memory copy or the
+// global image), prefix-table descriptors at pt and byte classes at cls.
+template <bool LEAN>
+__device__ __forceinline__ void tile_run(const MatchParams& p, const TileDev* t, const uint8_t* ib,
+                                         const PrefixTableDev* pt, const uint8_t* cls,
+                                         TileRun& tr) {
+  TileView& tv = tr.tv;
+  tv.succ = reinterpret_cast<const uint4*>(ib);
+  tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
+  tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
+  tv.sticky = !LEAN && t->nsticky > 0 ? reinterpret_cast<const uint32_t*>(ib + t->off_sticky)
+                                        : nullptr;
+  tv.cls = cls;
+  tv.t = t;
+  tv.pt = pt;
+  tv.cw = t->cw;
+  tv.narrow = t->narrow;
+  tv.fused = t->fused;
+  tv.nlive = (uint32_t)t->nlive;
+  tv.rep_levels = 0u;
+  for (int d = 0; d < kMaxDepth; d++) tv.rep_levels |= (pt[d].has_reports ? 1u : 0u) << d;
+  tr.depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
+  tr.batch = tr.depth == 0 ? t->inj_batch0 : t->inj_batch;
+  // short table lists, no sticky states: two positions per lane per injection
+  tr.wide_inject = tr.depth > 0 && !tv.sticky && tr.batch == 32;
+  // Without sticky states registered during the window (plain tiles
+  // without them, layered tiles), the last depth - 1 positions of a window
+  // are injected at the start of the next one (from look-behind bytes), so
+  // that every position but the unit's last ones gets the full table depth.
+  tr.layered = !LEAN && t->phase == 2;
+  tr.defer = (tr.depth > 1 && (!tv.sticky || tr.layered)) ? tr.depth - 1 : 0;
+}
+
+// Two kinds of work per launch:
+//  * tasks (consecutive units of one tile whose image fits shared memory):
+//    a CTA stages the image once and its warps take the task's units; the
+//    CTA waits for all of them before the next task replaces the image;
+//  * free units (tiles read in place through L2): every warp takes the next
+//    unit from a global cursor on its own and reads the tile's descriptors
+//    from global memory, so no warp waits for another.
+// CTAs take tasks until none is left, then free units. LEAN kernels serve
+// launches whose tiles have no sticky states and are plain (no activation or
+// layered pass): that code is compiled out, for a smaller hot loop.
+template <int PRIV, bool LEAN>
 __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   __shared__ int s_task;
@@ -1177,59 +1230,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     return bytes;
   };
 
-  while (true) {
-    if (threadIdx.x == 0) s_task = (int)atomicAdd(p.task_counter, 1u);
-    __syncthreads();
-    const int task = s_task;
-    if (task >= p.ntasks) break;
-    const TaskDev tk = p.tasks[task];
-    const TileDev* t = &p.tiles[tk.tile];
-    const bool fits = t->image_bytes <= p.image_region;
-    if (fits && staged != tk.tile) {  // stage the tile image (all warps are past the last task)
-      const uint4* src = reinterpret_cast<const uint4*>(t->image);
-      uint4* dst = reinterpret_cast<uint4*>(image);
-      for (int i = threadIdx.x; i < t->image_bytes / 16; i += kCtaThreads) dst[i] = __ldg(src + i);
-      staged = tk.tile;
-    }
-    {  // the tile's prefix-table descriptors, read at every injection, and its byte classes
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(t->pt);
-      uint32_t* dst = reinterpret_cast<uint32_t*>(s_pt);
-      for (int i = threadIdx.x; i < (int)(sizeof(s_pt) / 4); i += kCtaThreads) dst[i] = src[i];
-      if (threadIdx.x < 64)
-        reinterpret_cast<uint32_t*>(s_cls)[threadIdx.x] =
-            __ldg(reinterpret_cast<const uint32_t*>(t->image + t->off_cls) + threadIdx.x);
-    }
-    if (threadIdx.x == 0) s_next = (unsigned)tk.ubegin;
-    __syncthreads();
-    TileView tv;
-    const uint8_t* ib = fits ? image : t->image;
-    tv.succ = reinterpret_cast<const uint4*>(ib);
-    tv.succ2 = reinterpret_cast<const uint2*>(ib);
-    tv.cmask = reinterpret_cast<const uint32_t*>(ib + t->off_cmask);
-    tv.rep = reinterpret_cast<const uint32_t*>(ib + t->off_rep);
-    tv.sticky = t->nsticky > 0 ? reinterpret_cast<const uint32_t*>(ib + t->off_sticky) : nullptr;
-    tv.cls = s_cls;
-    tv.t = t;
-    tv.pt = s_pt;
-    tv.cw = t->cw;
-    tv.narrow = t->narrow;
-    tv.fused = t->fused;
-    tv.nlive = (uint32_t)t->nlive;
-    tv.rep_levels = 0u;
-    for (int d = 0; d < kMaxDepth; d++) tv.rep_levels |= (s_pt[d].has_reports ? 1u : 0u) << d;
-    const int depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
-    const int batch = depth == 0 ? t->inj_batch0 : t->inj_batch;
-    // short table lists, no sticky states: two positions per lane per injection
-    const bool wide_inject = depth > 0 && !tv.sticky && batch == 32;
-    const bool translate = t->cw != 8;
-    // Without sticky states registered during the window (plain tiles
-    // without them, layered tiles), the last depth - 1 positions of a window
-    // are injected at the start of the next one (from look-behind bytes), so
-    // that every position but the unit's last ones gets the full table depth.
-    const bool layered = t->phase == 2;
-    const int defer = (depth > 1 && (!tv.sticky || layered)) ? depth - 1 : 0;
-    // sticky list: shared memory, or global memory for layered tiles with
-    // more slots than that holds
+  // sticky list of the tile: shared memory, or global memory for layered
+  // tiles with more slots than that holds
+  auto sticky_lists = [&](const TileDev* t, bool layered) {
     if (layered && t->nact > kStickyCap && p.stk_g_cap >= t->nact) {
       ws.stk_s = p.stk_g + (size_t)slot * 2 * p.stk_g_cap;
       ws.stk_q = ws.stk_s + p.stk_g_cap;
@@ -1239,178 +1242,273 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       ws.stk_q = stk_smem + kStickyCap;
       w.stk_cap = kStickyCap;
     }
+  };
 
-    while (!dead) {
-      unsigned uid = 0;
-      if (lane == 0) uid = atomicAdd(&s_next, 1u);
-      uid = __shfl_sync(kFull, uid, 0);
-      if (uid >= (unsigned)tk.uend) break;
-      const UnitDev un = p.units[uid];
-      const unsigned long long work0 = n_expanded + n_injected;  // per-unit trace
-      UnitCtx c;
-      c.hi = un.hi;
-      c.emit_lo = un.emit_lo;
-      w.nstk = 0;  // sticky states are per unit
-      w.key_hi = un.key_hi;
-      w.base = (uint32_t)un.base;
-      w.act = t->phase == 1 ? p.act + un.act_row : nullptr;
-      if (layered) {
-        // sticky states whose first match (from the activation pass; the
-        // segment's matched slots are listed at act_list) comes before the
-        // unit's end: active from there on; a reporting one also reports at
-        // its first match
-        const uint32_t n = p.act_cnt[un.act_rowid];
-        bool rep_any = false;
-        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
-          const uint32_t i = i0 + lane;
-          const uint32_t slot = i < n ? p.act_list[un.act_row + i] : 0u;
-          const uint32_t f = i < n ? p.act[un.act_row + slot] : kNoAct;
-          const int64_t q = un.base + (int64_t)f;
-          const bool ok = f != kNoAct && q < c.hi;
-          const unsigned m = __ballot_sync(kFull, ok);
-          const uint32_t sv = ok ? __ldg(t->act_local + slot) : 0u;
-          if (ok) {
-            const int k = w.nstk + __popc(m & lanemask_lt(lane));
-            if (k < w.stk_cap) {
-              ws.stk_s[k] = slot;
-              ws.stk_q[k] = (uint32_t)q;
-            } else {
-              atomicOr(p.err, kErrQueue);
-            }
+  // matches unit uid of tile t (warp-collective)
+  auto run_unit = [&](unsigned uid, const TileDev* t, const TileRun& tr) {
+    const TileView& tv = tr.tv;
+    const int depth = tr.depth, batch = tr.batch, defer = tr.defer;
+    const bool layered = tr.layered, wide_inject = tr.wide_inject;
+    const UnitDev un = p.units[uid];
+    const unsigned long long work0 = n_expanded + n_injected;  // per-unit trace
+    UnitCtx c;
+    c.hi = un.hi;
+    c.emit_lo = un.emit_lo;
+    w.nstk = 0;  // sticky states are per unit
+    w.key_hi = un.key_hi;
+    w.base = (uint32_t)un.base;
+    w.act = !LEAN && t->phase == 1 ? p.act + un.act_row : nullptr;
+    if (layered) {
+      // sticky states whose first match (from the activation pass; the
+      // segment's matched slots are listed at act_list) comes before the
+      // unit's end: active from there on; a reporting one also reports at
+      // its first match
+      const uint32_t n = p.act_cnt[un.act_rowid];
+      bool rep_any = false;
+      for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t sl = i < n ? p.act_list[un.act_row + i] : 0u;
+        const uint32_t f = i < n ? p.act[un.act_row + sl] : kNoAct;
+        const int64_t q = un.base + (int64_t)f;
+        const bool ok = f != kNoAct && q < c.hi;
+        const unsigned m = __ballot_sync(kFull, ok);
+        const uint32_t sv = ok ? __ldg(t->act_local + sl) : 0u;
+        if (ok) {
+          const int k = w.nstk + __popc(m & lanemask_lt(lane));
+          if (k < w.stk_cap) {
+            ws.stk_s[k] = sl;
+            ws.stk_q[k] = (uint32_t)q;
+          } else {
+            atomicOr(p.err, kErrQueue);
           }
-          w.nstk = min(w.nstk + __popc(m), w.stk_cap);
-          const bool rs = ok && is_report(tv, sv);
-          rep_any |= rs;
-          const bool rep = rs && q >= c.emit_lo;
-          emit_report(p, ws, w, lane, rep, rep ? __ldg(t->sid + sv) : 0u, (uint32_t)q);
         }
-        w.stk_rep = __any_sync(kFull, rep_any);
+        w.nstk = min(w.nstk + __popc(m), w.stk_cap);
+        const bool rs = ok && is_report(tv, sv);
+        rep_any |= rs;
+        const bool rep = rs && q >= c.emit_lo;
+        emit_report(p, ws, w, lane, rep, rep ? __ldg(t->sid + sv) : 0u, (uint32_t)q);
+      }
+      w.stk_rep = __any_sync(kFull, rep_any);
+      __syncwarp();
+    }
+    int cur = 0;
+    uint32_t nbytes[2], skip[2];
+    if ((int32_t)uid != p.skip_copy_unit) {
+      nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
+    } else {  // test hook: nothing is in flight, the first wait gives up
+      nbytes[0] = 0u;
+      skip[0] = 0u;
+    }
+    int64_t inj_pos = un.lo;  // next position for always-active injection
+    for (int64_t wb = un.lo; wb < c.hi; wb += W) {
+      const int64_t we = min(wb + (int64_t)W, c.hi);
+      c.wb = wb;
+      c.wlen = (int)(we - wb);
+      c.iend = we == c.hi ? c.wlen : c.wlen - defer;
+      if (!mbar_wait(&ws.bar[cur], phase[cur], p.wait_rounds)) {
+        if (lane == 0) atomicOr(p.err, kErrTimeout);
+        dead = true;
+        break;
+      }
+      phase[cur] ^= 1u;
+      pending[cur] = false;
+      // bytes -> class ids, in place (every tile keys its tables by its own classes)
+      for (uint32_t i = lane; i < nbytes[cur]; i += 32) ws.in[cur][i] = tv.cls[ws.in[cur][i]];
+      __syncwarp();
+      if (we < c.hi)
+        nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi, (int)min((int64_t)defer, we - un.lo), skip[cur ^ 1]);
+      c.in = ws.in[cur] + skip[cur];
+      // carried states: matched at wb
+      w.top = 0;
+      if (w.ncarry > 0) {
+        for (int i = lane; i < w.ncarry; i += 32) {
+          const uint32_t u = w.carry[i];
+          w.marks[u >> 5] = 0u;
+          store_entry(p, ws, w, i, u << kEntryPosBits);
+        }
+        const int nc = w.ncarry;
+        w.ncarry = 0;
+        grow_stack(p, w, nc);
         __syncwarp();
       }
-      int cur = 0;
-      uint32_t nbytes[2], skip[2];
-      if ((int32_t)uid != p.skip_copy_unit) {
-        nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
-      } else {  // test hook: nothing is in flight, the first wait gives up
-        nbytes[0] = 0u;
-        skip[0] = 0u;
+      // start-of-data states at the unit's first position (ngap_buffer.cu:613-631)
+      if (wb == un.lo && (un.flags & 1u)) {
+        const uint32_t s0 = c.in[0];
+        for (int i0 = 0; i0 < t->nstart; i0 += 32) {
+          const int i = i0 + lane;
+          const uint32_t v = i < t->nstart ? __ldg(t->start + i) : 0u;
+          const bool ok = i < t->nstart && accepts(tv, v, s0);
+          const bool rep = ok && is_report(tv, v) && un.lo >= c.emit_lo;
+          emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v)) : 0u, (uint32_t)un.lo);
+          const bool need = ok && un.lo + 1 < c.hi;
+          bool reg = false;
+          if (layered)  // already registered from the activation pass
+            reg = is_sticky(tv, v);
+          else if (tv.sticky)
+            reg = register_each(p, ws, w, tv, c, lane, need && is_sticky(tv, v), v, un.lo, wb);
+          push_entry(p, ws, w, lane, need && !reg, v << kEntryPosBits);
+        }
       }
-      int64_t inj_pos = un.lo;  // next position for always-active injection
-      for (int64_t wb = un.lo; wb < c.hi; wb += W) {
-        const int64_t we = min(wb + (int64_t)W, c.hi);
-        c.wb = wb;
-        c.wlen = (int)(we - wb);
-        c.iend = we == c.hi ? c.wlen : c.wlen - defer;
-        if (!mbar_wait(&ws.bar[cur], phase[cur], p.wait_rounds)) {
-          if (lane == 0) atomicOr(p.err, kErrTimeout);
-          dead = true;
+      // next window offset to inject: negative for positions deferred from
+      // the previous window (at most `defer` of them)
+      int cursor = (int)(inj_pos - wb);
+      // layered tiles: next window offset of the sticky states' work
+      int scur = layered && w.nstk > 0 ? 0 : c.wlen;
+      while (true) {
+        // inject only when the overflow stack is empty, so that it holds at
+        // most one batch's excess
+        if (w.top < kInjectLow && w.ovf_n == 0) {
+          if (cursor < c.iend) {
+            if (wide_inject) {
+              inject_aas2(p, ws, w, tv, c, lane, cursor, 2 * batch, depth, n_injected);
+              cursor += 2 * batch;
+            } else if (LEAN) {
+              inject_aas(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
+              cursor += batch;
+            } else {
+              inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
+              cursor += batch;
+            }
+            continue;
+          }
+          if (!LEAN && scur < c.wlen) {
+            layered_sticky_positions(p, ws, w, tv, c, lane, scur);
+            scur += 32;
+            continue;
+          }
+        }
+        if (w.top == 0) {
+          if (w.ovf_n > 0) {  // refill from the overflow stack
+            const int m = min(w.ovf_n, kStackCap);
+            for (int i = lane; i < m; i += 32) ws.stack[i] = w.ovf[w.ovf_n - m + i];
+            w.ovf_n -= m;
+            w.top = m;
+            __syncwarp();
+            continue;
+          }
+          if (cursor < c.iend || (!LEAN && scur < c.wlen)) continue;
           break;
         }
-        phase[cur] ^= 1u;
-        pending[cur] = false;
-        if (translate) {  // bytes -> class ids, in place
-          for (uint32_t i = lane; i < nbytes[cur]; i += 32) ws.in[cur][i] = tv.cls[ws.in[cur][i]];
-        }
-        __syncwarp();
-        if (we < c.hi)
-          nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi, (int)min((int64_t)defer, we - un.lo), skip[cur ^ 1]);
-        c.in = ws.in[cur] + skip[cur];
-        // carried states: matched at wb
-        w.top = 0;
-        if (w.ncarry > 0) {
-          for (int i = lane; i < w.ncarry; i += 32) {
-            const uint32_t u = w.carry[i];
-            w.marks[u >> 5] = 0u;
-            store_entry(p, ws, w, i, u << kEntryPosBits);
-          }
-          const int nc = w.ncarry;
-          w.ncarry = 0;
-          grow_stack(p, w, nc);
-          __syncwarp();
-        }
-        // start-of-data states at the unit's first position (ngap_buffer.cu:613-631)
-        if (wb == un.lo && (un.flags & 1u)) {
-          const uint32_t s0 = c.in[0];
-          for (int i0 = 0; i0 < t->nstart; i0 += 32) {
-            const int i = i0 + lane;
-            const uint32_t v = i < t->nstart ? __ldg(t->start + i) : 0u;
-            const bool ok = i < t->nstart && accepts(tv, v, s0);
-            const bool rep = ok && is_report(tv, v) && un.lo >= c.emit_lo;
-            emit_report(p, ws, w, lane, rep, rep ? (__ldg(t->sid + v)) : 0u,
-                        (uint32_t)un.lo);
-            const bool need = ok && un.lo + 1 < c.hi;
-            bool reg = false;
-            if (layered)  // already registered from the activation pass
-              reg = is_sticky(tv, v);
-            else if (tv.sticky)
-              reg = register_each(p, ws, w, tv, c, lane, need && is_sticky(tv, v), v, un.lo, wb);
-            push_entry(p, ws, w, lane, need && !reg, v << kEntryPosBits);
-          }
-        }
-        // next window offset to inject: negative for positions deferred from
-        // the previous window (at most `defer` of them)
-        int cursor = (int)(inj_pos - wb);
-        // layered tiles: next window offset of the sticky states' work
-        int scur = layered && w.nstk > 0 ? 0 : c.wlen;
-        while (true) {
-          // inject only when the overflow stack is empty, so that it holds at
-          // most one batch's excess
-          if (w.top < kInjectLow && w.ovf_n == 0) {
-            if (cursor < c.iend) {
-              if (wide_inject) {
-                inject_aas2(p, ws, w, tv, c, lane, cursor, 2 * batch, depth, n_injected);
-                cursor += 2 * batch;
-              } else {
-                inject(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
-                cursor += batch;
-              }
-              continue;
-            }
-            if (scur < c.wlen) {
-              layered_sticky_positions(p, ws, w, tv, c, lane, scur);
-              scur += 32;
-              continue;
-            }
-          }
-          if (w.top == 0) {
-            if (w.ovf_n > 0) {  // refill from the overflow stack
-              const int m = min(w.ovf_n, kStackCap);
-              for (int i = lane; i < m; i += 32) ws.stack[i] = w.ovf[w.ovf_n - m + i];
-              w.ovf_n -= m;
-              w.top = m;
-              __syncwarp();
-              continue;
-            }
-            if (cursor < c.iend || scur < c.wlen) continue;
-            break;
-          }
-          if (PRIV == 0 && !tv.sticky)
-            expand_step2(p, ws, w, tv, c, lane, n_expanded);
-          else
-            expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
-        }
-        inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
-        cur ^= 1;
+        if (PRIV == 0 && (LEAN || !tv.sticky))
+          expand_step2(p, ws, w, tv, c, lane, n_expanded);
+        else
+          expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
       }
-      if (p.unit_work) {  // worklist work of this unit (all lanes)
-        unsigned long long d = n_expanded + n_injected - work0;
+      inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
+      cur ^= 1;
+    }
+    if (p.unit_work) {  // worklist work of this unit (all lanes)
+      unsigned long long d = n_expanded + n_injected - work0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
-        if (lane == 0) p.unit_work[uid] = d;
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+      if (lane == 0) p.unit_work[uid] = d;
+    }
+    if (dead) {
+      for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;
+      w.ncarry = w.top = w.ovf_n = 0;
+      // wait (bounded) for any copy still in flight before giving up on this warp
+      for (int b = 0; b < 2; b++)
+        if (pending[b]) {
+          mbar_wait(&ws.bar[b], phase[b], p.wait_rounds);
+          pending[b] = false;
+        }
+      __syncwarp();
+    }
+  };
+
+  // One loop, one call of run_unit: the next unit comes from the CTA's
+  // current task (staged tiles; a new task after a CTA barrier once the
+  // current one is exhausted) until no task is left, then from the free
+  // units, warp by warp. Every warp of a CTA takes the same barriers: a warp
+  // that gave up (dead) still waits for its CTA's tasks to end.
+  bool tasks_left = p.ntasks > 0;
+  bool free_ready = false;
+  bool need_task = true;
+  bool task_fits = false;
+  int task_end = 0;
+  const TileDev* task_tile = nullptr;
+  while (true) {
+    unsigned uid = 0;
+    const TileDev* t = nullptr;
+    if (tasks_left) {
+      if (need_task) {
+        __syncthreads();  // every warp is done with the last task before its image is replaced
+        if (threadIdx.x == 0) s_task = (int)atomicAdd(p.task_counter, 1u);
+        __syncthreads();
+        const int task = s_task;
+        if (task >= p.ntasks) {
+          tasks_left = false;
+          continue;
+        }
+        const TaskDev tk = p.tasks[task];
+        t = &p.tiles[tk.tile];
+        const bool fits = t->image_bytes <= p.image_region;
+        if (fits && staged != tk.tile) {  // stage the tile image
+          const uint4* src = reinterpret_cast<const uint4*>(t->image);
+          uint4* dst = reinterpret_cast<uint4*>(image);
+          for (int i = threadIdx.x; i < t->image_bytes / 16; i += kCtaThreads) dst[i] = __ldg(src + i);
+          staged = tk.tile;
+        }
+        {  // the tile's prefix-table descriptors, read at every injection, and its byte classes
+          const uint32_t* src = reinterpret_cast<const uint32_t*>(t->pt);
+          uint32_t* dst = reinterpret_cast<uint32_t*>(s_pt);
+          for (int i = threadIdx.x; i < (int)(sizeof(s_pt) / 4); i += kCtaThreads) dst[i] = src[i];
+          if (threadIdx.x < 64)
+            reinterpret_cast<uint32_t*>(s_cls)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(t->image + t->off_cls) + threadIdx.x);
+        }
+        if (threadIdx.x == 0) s_next = (unsigned)tk.ubegin;
+        __syncthreads();
+        task_tile = t;
+        task_fits = fits;
+        task_end = tk.uend;
+        need_task = false;
       }
       if (dead) {
-        for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;
-        w.ncarry = w.top = w.ovf_n = 0;
-        // wait (bounded) for any copy still in flight before giving up on this warp
-        for (int b = 0; b < 2; b++)
-          if (pending[b]) {
-            mbar_wait(&ws.bar[b], phase[b], p.wait_rounds);
-            pending[b] = false;
-          }
-        __syncwarp();
+        need_task = true;
+        continue;
       }
+      if (lane == 0) uid = atomicAdd(&s_next, 1u);
+      uid = __shfl_sync(kFull, uid, 0);
+      if (uid >= (unsigned)task_end) {
+        need_task = true;
+        continue;
+      }
+      t = task_tile;
+    } else {
+      if (!free_ready) {  // CTA-uniform: every warp of the CTA has left the tasks
+        if (p.free_tile >= 0) {  // one tile for all free units: its descriptors in shared memory
+          const TileDev* ft = &p.tiles[p.free_tile];
+          const uint32_t* src = reinterpret_cast<const uint32_t*>(ft->pt);
+          uint32_t* dst = reinterpret_cast<uint32_t*>(s_pt);
+          for (int i = threadIdx.x; i < (int)(sizeof(s_pt) / 4); i += kCtaThreads) dst[i] = src[i];
+          if (threadIdx.x < 64)
+            reinterpret_cast<uint32_t*>(s_cls)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(ft->image + ft->off_cls) + threadIdx.x);
+          __syncthreads();
+        }
+        free_ready = true;
+      }
+      if (dead || p.nfree <= 0) break;
+      unsigned k = 0;
+      if (lane == 0) k = atomicAdd(p.free_cursor, 1u);
+      k = __shfl_sync(kFull, k, 0);
+      if (k >= (unsigned)p.nfree) break;
+      uid = (unsigned)p.free_begin + k;
+      t = &p.tiles[p.units[uid].tile];
     }
-    __syncthreads();  // every warp is done with this task before the image is replaced
+    // the unit's view of its tile (rebuilt per unit, so that it is not live
+    // across units): the staged image and shared descriptors of the task, or
+    // for free units the global image and descriptors, read in place
+    TileRun tr;
+    if (tasks_left)
+      tile_run<LEAN>(p, t, task_fits ? image : t->image, s_pt, s_cls, tr);
+    else if (p.free_tile >= 0 && t == p.tiles + p.free_tile)
+      tile_run<LEAN>(p, t, t->image, s_pt, s_cls, tr);
+    else
+      tile_run<LEAN>(p, t, t->image, t->pt, t->image + t->off_cls, tr);
+    sticky_lists(t, tr.layered);
+    run_unit(uid, t, tr);
   }
   flush_reports(p, ws, w, lane);
 #pragma unroll

@@ -466,12 +466,11 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
   if (n == 0) return true;
   t.cw = class_words(part.n);
   t.cls.resize(256);
-  if (t.cw == 8) {  // more than 64 classes: classes are the bytes themselves
-    t.ncls = 256;
-    t.nlive = 256;
-    for (int b = 0; b < 256; b++) t.cls[b] = (uint8_t)b;
-  } else {
-    // bytes no state accepts share one (dead) class; number it last
+  {
+    // bytes no state accepts share one (dead) class; number it last. More
+    // than 64 classes take 8 mask words, but the keys still count only the
+    // live classes, so prefix tables reach one more level within 32-bit keys
+    // than keys over raw bytes (95 printable classes: depth 4 instead of 3)
     uint32_t any[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (size_t ci = 0; ci < ccs.size(); ci++) {
       const CcInfo& c = ccs[ci];

@@ -140,9 +140,9 @@ def test_prefix_tables_match_restated_semantics(case):
     if case == "hamming":
         anml, data = W.hamming_set(seed=2, n_patterns=3, k=8, input_len=1 << 12, plant_every=1 << 9)
         g, kw = 1, dict(precompute_depth=5, tile_mode="shared")
-    elif case == "literal":  # 95 classes: byte keys (nlive 256), level 3 hashed
+    elif case == "literal":  # 95 live classes (8 mask words): keys base 95, level 4 hashed
         anml, data = W.literal_set(seed=1, input_len=1 << 12, plant_every=1 << 9)
-        g, kw = 1, dict(precompute_depth=3, tile_mode="shared")
+        g, kw = 1, dict(precompute_depth=4, tile_mode="shared")
     elif case == "levenshtein":
         anml, data = W.levenshtein_set(seed=3, n_patterns=2, k=8, input_len=1 << 12,
                                        plant_every=1 << 9)
@@ -156,7 +156,7 @@ def test_prefix_tables_match_restated_semantics(case):
     assert len(tiles) == 1 and tiles[0]["num_ccs"] == sum(len(v.cc_begin) - 1 for v in views)
     t = tiles[0]
     if case == "literal":
-        assert t["nlive"] == 256 and t["dense_levels"] & 4 == 0  # level 3 is hashed
+        assert t["nlive"] == 95 and t["depth"] == 4 and t["dense_levels"] & 8 == 0
     else:
         assert t["dense_levels"] == (1 << t["depth"]) - 1
     nonempty = 0
