@@ -577,7 +577,7 @@ class Suite:
         self.setup_s = time.time() - t0
 
 
-def stream_parity(suite, reps, sids, nsample=48, prefix=64 << 10, seed=0):
+def stream_parity(suite, reps, sids, nsample=32, prefix=32 << 10, seed=0):
     """Per-stream parity on a random sample: each sampled stream's reports at
     offsets below `prefix` against the oracle on the stream's first `prefix`
     bytes (a report at offset q depends only on the stream's bytes up to q)."""
@@ -618,7 +618,11 @@ def batched_part(args, warmup, suite, local_rank, steps):
     s = suite
     eng, ts = s.eng, s.ts
     t0 = time.time()
-    best, tuned = autotune.autotune(eng, ts, s.data, s.offsets, s.lengths, s.nfa_of, frac=0.01)
+    if args.batched_params:  # fixed parameters (profiling): no autotuning launches
+        best, tuned = json.loads(args.batched_params), []
+    else:
+        best, tuned = autotune.autotune(eng, ts, s.data, s.offsets, s.lengths, s.nfa_of,
+                                        frac=0.01)
     tune_s = time.time() - t0
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -711,6 +715,9 @@ def batched_part(args, warmup, suite, local_rank, steps):
     return out
 
 
+# chunk lengths of the predicting schedulers (cost_model.chunk_for)
+SERVE_CHUNKS = dict(adapt_chunks=True, rho_ref=1.0, base_chunk=512, chunk_lo=64, chunk_hi=2048)
+
 SERVE_DESC = ("Poisson requests at 2000/s, NFA uniform over the 16 of the batched suite, "
               "length log-normal (median 64 KiB, sigma 1.5, at most 4 MiB), 2 engine slots, "
               "8 GiB device-memory budget")
@@ -748,28 +755,29 @@ def serving_part(args, warmup, suite, steps, step_s=0.25):
              "learned": sv.Predictor("learned", s.tables, lm)}
     servers = {}
     for name, pred in preds.items():
-        q, heavy = 0, None
+        q = 0
         if pred is not None:
-            dens = pred.density(warm)
-            q = cm.queue_for(float(np.max(dens)))
-            heavy = float(np.quantile(dens * np.array([len(r.data) for r in warm]), 0.9))
+            q = cm.queue_for(float(np.max(pred.density(warm))))
         srv = sv.Server(s.ts, predictor=pred, slots=2, budget=8 << 30, queue_capacity=q,
-                        isolate=pred is not None, heavy_work=heavy, adapt_chunks=False)
+                        **(SERVE_CHUNKS if pred is not None else {}))
         srv.run([sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in warm])
-        servers[name] = (srv, q, heavy)
+        servers[name] = (srv, q)
     lat = {name: [] for name in preds}
     served, launches, clk_all, dev_ms, d2h, results = {}, 0, None, 0.0, 0, {}
     for rnd in range(2):  # two interleaved rounds of the three schedulers
-        for name, (srv, q, heavy) in servers.items():
+        for name, (srv, q) in servers.items():
             srv.batches.clear()
             srv.launches = 0
             rs = [sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in reqs]
             with ClockSampler(0) as clk:
                 m = srv.run(rs)
             launches += srv.launches
+            dev = np.array([b[3] for b in srv.batches]) if srv.batches else np.zeros(1)
             lat[name].append({"p50_ms": m["p50_ms"], "p99_ms": m["p99_ms"],
                               "mean_ms": m["mean_ms"], "batches": m["batches"],
-                              "rejected": m["rejected"]})
+                              "rejected": m["rejected"],
+                              "batch_device_ms_p50": float(np.percentile(dev, 50)),
+                              "batch_device_ms_p99": float(np.percentile(dev, 99))})
             served.setdefault(name, []).append(m["MBps"])
             if rnd == 1:
                 results[name] = rs
@@ -784,9 +792,9 @@ def serving_part(args, warmup, suite, steps, step_s=0.25):
                for k in ("static", "learned") for i in range(len(reqs)))
     rng = np.random.default_rng(3)
     ok, nchk, t1 = True, 0, time.time()
-    for i in sorted(rng.choice(len(reqs), size=min(48, len(reqs)), replace=False)):
+    for i in sorted(rng.choice(len(reqs), size=min(24, len(reqs)), replace=False)):
         r = results["learned"][int(i)]
-        L = min(len(r.data), 64 << 10)
+        L = min(len(r.data), 16 << 10)
         want, _ = oracle.match(s.groups[r.nfa].views(), r.data[:L], 1, L,
                                nthreads=os.cpu_count() or 1)
         ok &= bool(np.array_equal(r.reports[(r.reports & M32) < np.uint64(L)], want))
@@ -805,16 +813,17 @@ def serving_part(args, warmup, suite, steps, step_s=0.25):
             "learned_vs_static": {
                 "p99_ratio": summary["learned"]["p99_ms"] / summary["static"]["p99_ms"],
                 "p50_ratio": summary["learned"]["p50_ms"] / summary["static"]["p50_ms"]},
-            "scheduler": "default: batches in arrival order; static / learned: the request's "
-                         "work predicted at arrival (density x length) sends requests above "
-                         "the 90th percentile of the warm-up predictions to a heavy lane "
-                         "batched apart on the second slot; queue sized from the densest "
-                         "prediction",
-            "heavy_work_threshold": {k: servers[k][2] for k in ("static", "learned")},
+            "scheduler": "default: the engine's chunks (about 2 KiB); static / learned: "
+                         "each request's density (worklist entries per byte) predicted when a "
+                         "slot is free, chunk = 512 x (1 + 1) / (1 + density) clamped to "
+                         "[64, 2048] bytes, so that a batch's longest unit stays short; "
+                         "batches in arrival order on 2 slots; queue sized from the densest "
+                         "warm-up prediction",
+            "chunk_policy": SERVE_CHUNKS,
             "frontier_prediction_rel_err": err,
             "gpu_launches": launches, "clocks": clk_all,
             "parity_vs_oracle": {"bit_exact": bool(ok and same), "same_under_every_scheduler":
-                                 bool(same), "requests_checked": nchk, "prefix_bytes": 64 << 10,
+                                 bool(same), "requests_checked": nchk, "prefix_bytes": 16 << 10,
                                  "oracle_seconds": round(time.time() - t1, 1)},
             "e2e": {"value": summary["learned"]["served_mbps"], "unit": "MB/s",
                     "h2d_bytes_per_step": int(total / max(1, steps)),
@@ -947,6 +956,8 @@ def main():
                          "max(1, 2 x this / steps) per step)")
     ap.add_argument("--segments", type=int, default=0,
                     help="match only the first N segments (smaller case for profiling)")
+    ap.add_argument("--batched-params", default="",
+                    help="JSON parameters of the batched launch instead of autotuning them")
     ap.add_argument("--streams", type=int, default=4096,
                     help="streams of the batched suite (fewer: a smaller case for profiling)")
     args = ap.parse_args()
@@ -981,12 +992,18 @@ def main():
         return
 
     dist = _dist_setup(world, local_rank)
+    t0 = time.time()
     line = run_plain(args, warmup, rank, world, local_rank, dist)
+    if rank == 0:
+        line["wall_seconds"] = {"plain": round(time.time() - t0, 1)}
     if rank == 0 and world == 1 and args.workload == "hamming_set" and not args.no_extras:
+        t1 = time.time()
         suite = Suite(local_rank)
         line["batched"] = batched_part(args, warmup, suite, local_rank, min(args.steps, 5))
-        line["batched"]["vs_plain_headline"] = line["batched"]["value"] / line["value"]
+        t2 = time.time()
         line["serving"] = serving_part(args, warmup, suite, args.steps)
+        line["wall_seconds"].update({"batched": round(t2 - t1, 1),
+                                     "serving": round(time.time() - t2, 1)})
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

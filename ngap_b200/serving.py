@@ -93,6 +93,28 @@ def host_features(data, window=cm.ENTROPY_WINDOW):
     return out
 
 
+def host_features_many(datas, window=cm.ENTROPY_WINDOW):
+    """host_features of several regions; row i equals host_features(datas[i]).
+    Regions of one common length that is a multiple of `window` (full 16 KiB
+    regions, the usual case) share one histogram pass over all their windows."""
+    out = np.zeros((len(datas), 258), np.float32)
+    full = [i for i, d in enumerate(datas) if len(d) == cm.REGION and cm.REGION % window == 0]
+    for i, d in enumerate(datas):
+        if not full or i not in set(full):
+            out[i] = host_features(d, window)
+    if full:
+        k, nwin = len(full), cm.REGION // window
+        block = np.stack([datas[i] for i in full]).reshape(k * nwin, window)
+        c = np.bincount((_window_base(k * nwin, window) + block.ravel()), minlength=k * nwin * 256)
+        c = c.reshape(k, nwin, 256)
+        q = c / window
+        h = -np.sum(q * np.log2(np.where(q > 0, q, 1.0)), axis=2)  # [k, nwin]
+        out[full, :256] = c.sum(axis=1) / cm.REGION
+        out[full, 256] = h.mean(axis=1) / 8
+        out[full, 257] = h.max(axis=1) / 8
+    return out
+
+
 _bases = {}
 
 
@@ -120,8 +142,8 @@ class Predictor:
         nf = np.array([r.nfa for r in reqs], dtype=np.int64)
         if self.kind != "learned":
             return self.static.predict(nf)
-        x = np.stack([np.concatenate([host_features(r.data[:cm.REGION]), self.nfeat[r.nfa]])
-                      for r in reqs]).astype(np.float32)
+        feats = host_features_many([r.data[:cm.REGION] for r in reqs])
+        x = np.concatenate([feats, self.nfeat[nf]], axis=1).astype(np.float32)
         return self.model.predict(nf, x, bf16=True)
 
 
@@ -191,10 +213,11 @@ class Server:
     against `budget` bytes. Engine buffers only grow (ngap_engine_memory), so
     a batch is launched on a slot only when what it would add to that
     engine (a larger input copy, a larger unit plan) keeps the total within
-    the budget. Each engine's fixed part (report buffers for `rep_cap`
-    reports, per-warp overflow stacks) is allocated by a one-stream warm-up
-    batch at construction, so it is counted from the start; a budget that
-    cannot hold the tables and those parts raises ValueError. A request that
+    the budget. Each engine's buffers (an input copy of max_batch_bytes,
+    report buffers for `rep_cap` reports, per-warp overflow stacks) are
+    allocated by a one-stream warm-up batch at construction, so they are
+    counted from the start and never grow while serving; a budget that
+    cannot hold the tables and those buffers raises ValueError. A request that
     can never be admitted (longer than max_batch_bytes, or needing more than
     the budget leaves with every engine as it is) is rejected at arrival:
     its `error` is set and it gets no reports.
@@ -230,8 +253,13 @@ class Server:
         self.batches = []               # (size, bytes, predicted work, device ms)
         self.launches = 0               # kernels launched by the served batches
         self.rejected = []              # requests that can never be admitted
-        for sl in self.slots:           # allocate each engine's fixed part now
-            sl.launch([Request(-1, 0, np.zeros(16, np.uint8), 0.0)], self._params())
+        # allocate each engine's buffers now, for the largest batch (an input
+        # copy of max_batch_bytes, report buffers, per-warp overflow stacks):
+        # a buffer that grew while serving would cost a cudaMalloc, which
+        # waits for the whole device
+        warm = Request(-1, 0, np.zeros(max(16, max_batch_bytes), np.uint8), 0.0)
+        for sl in self.slots:
+            sl.launch([warm], self._params())
             sl.finish(1)
         self.mem = [sl.memory() for sl in self.slots]
         if self.tables_bytes + sum(self._held(m) for m in self.mem) > budget:
@@ -296,43 +324,52 @@ class Server:
     def run(self, requests):
         """Serves requests (sorted by arrival) in real time; returns metrics.
 
-        Without isolation, batches take the queue in arrival order. With
-        isolation (a predictor and at least two slots), a request whose
-        predicted work (density x length) exceeds heavy_work goes to the heavy
-        queue: slot 0 serves only the light queue, the other slots the heavy
-        queue first and the light one when it is empty, so that light requests
-        never share a batch with (and wait for) a predicted-heavy one."""
+        Requests that arrived since the last pass of the loop are predicted
+        together (one model call, inside the clock, while earlier batches may
+        still run): their work (density x length) and, with adapt_chunks,
+        their chunk length. Without isolation, batches take the queue in arrival order.
+        With isolation (a predictor and at least two slots), a request whose
+        predicted work exceeds heavy_work goes to the heavy queue: slot 0
+        serves only the light queue, the other slots the heavy queue first
+        and the light one when it is empty, so that light requests never
+        share a batch with (and wait for) a predicted-heavy one."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        light, heavy, nxt = [], [], 0
+        pending, light, heavy, nxt = [], [], [], 0
         self._t0 = time.perf_counter()
-        while nxt < len(reqs) or light or heavy or any(b is not None for b in self.busy):
+        while (nxt < len(reqs) or pending or light or heavy
+               or any(b is not None for b in self.busy)):
             now = time.perf_counter() - self._t0
-            fresh = []
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
                 r = reqs[nxt]
                 nxt += 1
                 if self.admissible(r):
-                    fresh.append(r)
+                    pending.append(r)
                 else:
                     r.error = (f"request of {len(r.data)} bytes can never be admitted "
                                f"(max_batch_bytes {self.max_bytes}, budget {self.budget})")
                     r.done = now
                     self.rejected.append(r)
-            if self.pred is not None and fresh:  # predictions at arrival, inside the clock
-                rho = self.pred.density(fresh)
-                chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk, self.chunk_lo,
-                                      self.chunk_hi)
-                for r, d, c in zip(fresh, rho, chunks):
-                    r.pred_work = float(d) * len(r.data)
-                    r.chunk = int(c) if self.adapt_chunks else 0
-            for r in fresh:
-                if self.isolate and self.heavy_work is not None and r.pred_work > self.heavy_work:
-                    heavy.append(r)
-                else:
-                    light.append(r)
             for s, b in enumerate(self.busy):
                 if b is not None and self.slots[s].done():
                     self._finish(s)
+            # predict as soon as requests arrive (while slots may still be busy,
+            # so that the model's cost overlaps the device work), all of them
+            # in one call
+            if pending:
+                if self.pred is not None:  # one prediction for everything that arrived
+                    rho = self.pred.density(pending)
+                    chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk, self.chunk_lo,
+                                          self.chunk_hi)
+                    for r, d, c in zip(pending, rho, chunks):
+                        r.pred_work = float(d) * len(r.data)
+                        r.chunk = int(c) if self.adapt_chunks else 0
+                for r in pending:
+                    if (self.isolate and self.heavy_work is not None
+                            and r.pred_work > self.heavy_work):
+                        heavy.append(r)
+                    else:
+                        light.append(r)
+                pending = []
             for s in range(len(self.busy)):
                 if self.busy[s] is not None:
                     continue
@@ -348,7 +385,8 @@ class Server:
                         self.slots[s].launch(batch, self._params())
                         self.mem[s] = self.slots[s].memory()
                         self.busy[s] = (batch, now)
-            if not light and not heavy and nxt < len(reqs) and all(b is None for b in self.busy):
+            if (not pending and not light and not heavy and nxt < len(reqs)
+                    and all(b is None for b in self.busy)):
                 time.sleep(max(0.0, min(reqs[nxt].arrival - now, 0.0005)))
         return summarize([r for r in reqs if r.error is None], self.batches,
                          rejected=len(self.rejected))

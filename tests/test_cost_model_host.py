@@ -108,13 +108,13 @@ class FakeSlot:
         return [np.array([rid], np.int64) for rid in self.launched[-1]], 0.5, 3
 
 
-def _server(budget, max_bytes, slots=1, fixed=1000, tables=100):
+def _server(budget, max_bytes, slots=1, fixed=1000, tables=100, chunk_lo=1 << 30):
     made = []
 
     def factory(i):
         made.append(FakeSlot(fixed))
         return made[-1]
-    srv = sv.Server(None, slots=slots, budget=budget, max_batch_bytes=max_bytes, chunk_lo=1 << 30,
+    srv = sv.Server(None, slots=slots, budget=budget, max_batch_bytes=max_bytes, chunk_lo=chunk_lo,
                     slot_factory=factory, tables_bytes=tables)
     return srv, made
 
@@ -124,26 +124,27 @@ def _reqs(sizes):
 
 
 def test_serving_admission_counts_engine_buffers():
-    # tables 100 + fixed 1000 + the warm-up batch's input copy (16 B -> 80)
+    # tables 100 + fixed 1000 + the warm-up batch's input copy of max_batch_bytes
+    # (1000 B -> 1072): every engine buffer is allocated at construction
     srv, made = _server(budget=10_000, max_bytes=1000)
-    assert srv.held_bytes() == 100 + 1000 + 80
+    assert srv.held_bytes() == 100 + 1000 + 1072
     q = _reqs([400, 300, 200, 500])  # capped by max_batch_bytes, in arrival order
     assert [r.rid for r in srv._form(q, 0)] == [0, 1, 2] and [r.rid for r in q] == [3]
-    # held 1180; a batch adds its padded input beyond the 80 held and a unit
-    # plan of 80 B x (2 per stream): 400 B -> 384 + 160 = 544 (1724 <= 1800),
-    # 700 B in two streams -> 704 + 320 = 1024 (2204 > 1800)
-    srv, made = _server(budget=1800, max_bytes=10_000)
+    # held 100 + 1000 + 10072; a batch of n streams adds a unit plan of 80 B x 2n:
+    # two requests add 320 (within 400 of room), three 480
+    srv, made = _server(budget=100 + 1000 + 10_072 + 400, max_bytes=10_000)
     q = _reqs([400, 300, 200])
     got = srv._form(q, 0)
-    assert [r.rid for r in got] == [0] and len(q) == 2
-    with pytest.raises(ValueError):  # the fixed parts alone exceed the budget
-        _server(budget=1000, max_bytes=1000)
+    assert [r.rid for r in got] == [0, 1] and len(q) == 1
+    with pytest.raises(ValueError):  # the buffers alone exceed the budget
+        _server(budget=2000, max_bytes=1000)
 
 
 def test_serving_rejects_requests_that_never_fit():
-    # held 100 + 2 x 1080 = 2260; a lone request of n bytes adds (pad(n) - 80) + 160:
-    # 900 -> 1064 (3324 > 3000), 300 -> 444 (2704), 200 -> 352, 100 -> 256
-    srv, made = _server(budget=3000, max_bytes=1000, slots=2)
+    # held 100 + 2 x (1000 + 1072) = 4244, room 500; a lone request of n bytes
+    # adds a plan of 80 B x (n // 100 + 2): 900 -> 880 (never fits),
+    # 300 -> 400, 200 -> 320, 100 -> 240
+    srv, made = _server(budget=4244 + 500, max_bytes=1000, slots=2, chunk_lo=100)
     reqs = _reqs([300, 5000, 200, 900, 100])  # 5000 > max_batch_bytes; 900 > the budget
     m = srv.run(reqs)  # returns instead of waiting forever
     assert m["rejected"] == 2 and m["requests"] == 3
@@ -193,6 +194,7 @@ def test_autotune_search_with_fake_launches():
     assert len(calls) == 8 * 3 + 4
     with pytest.raises(ValueError):
         at.autotune(None, None, data, offsets, lengths, nfa_of, tile_grid=[{}], run=run)
+
 
 
 class FakePredictor:
