@@ -184,6 +184,8 @@ struct UnitCtx {
   int64_t wb, hi, emit_lo;
   int wlen;
   int iend;           // always-active injection covers window offsets below iend
+  int lim;            // hi - wb, capped: a window offset r has a next symbol when r + 1 < lim
+  int elo;            // emit_lo - wb, clamped: reports at window offsets >= elo are kept
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -674,7 +676,7 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
   uint32_t len[2];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    len[h] = (k[h] == kmax[h] && k[h] > 0 && c.wb + r[h] + k[h] < c.hi) ? (ve[h] - vb[h]) : 0u;
+    len[h] = (k[h] == kmax[h] && k[h] > 0 && r[h] + k[h] < c.lim) ? (ve[h] - vb[h]) : 0u;
     n_injected += len[h];
   }
   const uint32_t mine = len[0] + len[1];
@@ -1040,6 +1042,10 @@ __device__ __forceinline__ void expand_step(const MatchParams& p, WarpSmem& ws, 
 // sticky states and without privatization: both entries' successor records
 // are requested before either is used, so a warp keeps two L2 round trips in
 // flight per lane instead of one. Same results as two expand_step calls.
+// FUSED: the tile's records carry the successors' class masks (one 32-byte
+// record per state); the window arithmetic is 32-bit (UnitCtx::lim, elo)
+// and the rare report and carry paths are entered on one vote each.
+template <bool FUSED>
 __device__ __forceinline__ void expand_step2(const MatchParams& p, WarpSmem& ws, WarpRun& w,
                                              const TileView& tv, const UnitCtx& c, int lane,
                                              unsigned long long& n_expanded) {
@@ -1063,38 +1069,59 @@ __device__ __forceinline__ void expand_step2(const MatchParams& p, WarpSmem& ws,
 #pragma unroll
   for (int k = 0; k < 2; k++) {
     r[k] = (int)(e[k] & ((1u << kEntryPosBits) - 1));
-    go[k] = e[k] != kNoEntry && c.wb + r[k] + 1 < c.hi;
+    go[k] = e[k] != kNoEntry && r[k] + 1 < c.lim;
     sc[k] = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
     sm[k] = make_uint4(0u, 0u, 0u, 0u);
     s[k] = 0u;
     if (go[k]) {
       const uint32_t v = e[k] >> kEntryPosBits;
-      sc[k] = load_succ(tv, v);
-      if (tv.fused) sm[k] = load_smask(tv, v);
+      if (FUSED) {
+        sc[k] = tv.succ[(size_t)v * 2];
+        sm[k] = tv.succ[(size_t)v * 2 + 1];
+      } else {
+        sc[k] = load_succ(tv, v);
+      }
       s[k] = c.in[r[k] + 1];
     }
-    n_expanded += go[k];
   }
+  n_expanded += (unsigned)go[0] + (unsigned)go[1];
   bool ok[2][4], need[2], at_end[2];
+  bool rep = false, carry = false;
   int cnt = 0;
 #pragma unroll
   for (int k = 0; k < 2; k++) {
     const uint32_t u[4] = {sc[k].x, sc[k].y, sc[k].z, sc[k].w};
     const uint32_t um[4] = {sm[k].x, sm[k].y, sm[k].z, sm[k].w};
-    const int64_t q = c.wb + r[k];
+    bool rk = false;
 #pragma unroll
-    for (int j = 0; j < 4; j++) ok[k][j] = go[k] && succ_accepts(tv, u[j], um[j], s[k]);
-    report4(p, ws, w, tv, lane, ok[k], u, q + 1, q + 1 >= c.emit_lo);
-    need[k] = go[k] && q + 2 < c.hi;
-    at_end[k] = r[k] + 1 == c.wlen;
-    if (__any_sync(kFull, need[k] && at_end[k])) {
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        carry_state(p, w, lane, need[k] && at_end[k] && ok[k][j], u[j] & kIdMask);
+    for (int j = 0; j < 4; j++) {
+      ok[k][j] = go[k] && (FUSED ? ((um[j] >> s[k]) & 1u) != 0u : succ_accepts(tv, u[j], um[j], s[k]));
+      rk |= ok[k][j] && (u[j] >> 31);
     }
+    rep |= rk && r[k] + 1 >= c.elo;
+    need[k] = go[k] && r[k] + 2 < c.lim;
+    at_end[k] = r[k] + 1 == c.wlen;
+    carry |= need[k] && at_end[k];
     if (need[k] && !at_end[k]) {
 #pragma unroll
       for (int j = 0; j < 4; j++) cnt += ok[k][j];
+    }
+  }
+  if (__any_sync(kFull, rep)) {  // reports (rare): the warp-collective path per half
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint32_t u[4] = {sc[k].x, sc[k].y, sc[k].z, sc[k].w};
+      const int64_t q = c.wb + r[k];
+      report4(p, ws, w, tv, lane, ok[k], u, q + 1, r[k] + 1 >= c.elo);
+    }
+  }
+  if (__any_sync(kFull, carry)) {  // states landing on the next window's first position
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint32_t u[4] = {sc[k].x, sc[k].y, sc[k].z, sc[k].w};
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        carry_state(p, w, lane, need[k] && at_end[k] && ok[k][j], u[j] & kIdMask);
     }
   }
   int total;
@@ -1305,6 +1332,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       c.wb = wb;
       c.wlen = (int)(we - wb);
       c.iend = we == c.hi ? c.wlen : c.wlen - defer;
+      c.lim = (int)min(c.hi - wb, (int64_t)1 << 30);
+      c.elo = (int)max(min(c.emit_lo - wb, (int64_t)1 << 30), -((int64_t)1 << 30));
       if (!mbar_wait(&ws.bar[cur], phase[cur], p.wait_rounds)) {
         if (lane == 0) atomicOr(p.err, kErrTimeout);
         dead = true;
@@ -1389,10 +1418,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
           if (cursor < c.iend || (!LEAN && scur < c.wlen)) continue;
           break;
         }
-        if (PRIV == 0 && (LEAN || !tv.sticky))
-          expand_step2(p, ws, w, tv, c, lane, n_expanded);
-        else
+        if (PRIV == 0 && (LEAN || !tv.sticky)) {
+          if (tv.fused)
+            expand_step2<true>(p, ws, w, tv, c, lane, n_expanded);
+          else
+            expand_step2<false>(p, ws, w, tv, c, lane, n_expanded);
+        } else {
           expand_step<PRIV>(p, ws, w, tv, c, lane, cursor, n_expanded);
+        }
       }
       inj_pos = max(inj_pos, wb + c.iend);  // a batch may end past iend
       cur ^= 1;

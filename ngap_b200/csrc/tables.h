@@ -61,7 +61,7 @@ struct TableOpts {
   int max_warmup = 2048;            // longest acyclic path that still allows chunking
   int tile_mode = 0;                // 0 automatic, 1 shared-memory tiles, 2 global tiles
   bool layered = true;              // chunk CCs that are cyclic only through sticky self-loops
-  int64_t auto_global_table_bytes = 96 << 20;  // automatic depth, global tiles
+  int64_t auto_global_table_bytes = 192 << 20;  // automatic depth, global tiles
   int64_t global_table_entries = 32 << 20;     // list entries per table, global tiles
 };
 
