@@ -147,9 +147,23 @@ int plan_tiles(const char* fn, const ngap_groups* g, const ngap_table_opts* opts
 // [vb, ve) and [rb, re) of `key` in a prefix table, laid out as the matching
 // kernel reads it (dense offsets by key, or linear-probing hash slots
 // {key, list begin, report-list begin, list length << 16 | report length}).
+// As the kernel's pt_find; `one` receives the lone state of an inline1 key
+// (kNoSucc otherwise), whose list [vb, ve) is then empty.
 void table_find(const PrefixTableHost& t, uint32_t key, uint32_t& vb, uint32_t& ve, uint32_t& rb,
-                uint32_t& re) {
+                uint32_t& re, uint32_t& one) {
   vb = ve = rb = re = 0;
+  one = kNoSucc;
+  if (t.inline1) {
+    const uint32_t x = t.voff[key];
+    if (x == kHashEmpty) return;
+    if (x >> 31) {
+      vb = (x >> 6) & 0x1ffffffu;
+      ve = vb + (x & 63u);
+    } else {
+      one = x;
+    }
+    return;
+  }
   if (t.dense) {
     vb = t.voff[key];
     ve = t.voff[key + 1];
@@ -245,7 +259,12 @@ int ngap_tiles_lookup(const ngap_groups* g, const ngap_table_opts* opts, int til
       dead = dead || c >= L;  // a dead byte ends every path: no lookup
       key = key * L + c;
     }
-    if (!dead) table_find(pt, key, vb, ve, rb, re);
+    uint32_t one = kNoSucc;
+    if (!dead) table_find(pt, key, vb, ve, rb, re, one);
+    if (one != kNoSucc) {
+      if (nv < cap) ids[nv] = t.sid[one];
+      nv++;
+    }
     for (uint32_t j = vb; j < ve; j++, nv++)
       if (nv < cap) ids[nv] = t.sid[pt.vlist[j]];
     for (uint32_t j = rb; j < re; j++, nr++)

@@ -27,12 +27,18 @@ constexpr uint32_t kHashEmpty = 0xffffffffu;
 // {key, state-list begin, report-list begin, state-list length << 16 |
 // report-list length}; the reference binary-searches a sorted key array
 // (precompute_table.h:59-100).
+// inline1 (dense tables without report lists): voff holds one word per key
+// [space]: kHashEmpty for an empty list, the state itself (bit 31 clear) for
+// a list of one, else bit 31 | begin << 6 | length (2..63) into vlist; most
+// keys of a deep table have at most one state, so a lookup is one read.
 struct PrefixTableDev {
   int32_t dense = 0;
   uint32_t hmask = 0;               // hash capacity - 1
   int32_t cutoff = 0;
   int32_t has_reports = 0;          // any report list non-empty
-  const uint32_t* voff = nullptr;   // dense: state-list offsets [space + 1]
+  int32_t inline1 = 0;
+  int32_t pad = 0;
+  const uint32_t* voff = nullptr;   // dense: state-list offsets [space + 1], or inline1 words
   const uint32_t* roff = nullptr;   // dense: report-list offsets [space + 1] (if reports)
   const uint4* slots = nullptr;     // hashed: [hmask + 1]
   const uint32_t* vlist = nullptr;  // local states reached after d symbols

@@ -290,6 +290,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       const PrefixTableHost& ph = th.pt[k];
       PrefixTableDev& pd = d.pt[k];
       pd.dense = ph.dense ? 1 : 0;
+      pd.inline1 = ph.inline1 ? 1 : 0;
       pd.hmask = ph.hmask;
       pd.cutoff = ph.cutoff;
       pd.has_reports = ph.rlist.empty() ? 0 : 1;
@@ -1331,19 +1332,12 @@ int ngap_tables_stats_get(const ngap_tables* t, ngap_tables_stats* out) {
     st.depth = std::max(st.depth, th.depth);
     st.max_nlive = std::max(st.max_nlive, th.nlive);
     const PrefixTableHost& pt = th.pt[th.depth - 1];
-    st.list_entries += (int64_t)pt.vlist.size();
+    st.list_entries += pt.entries;
     st.cutoff += pt.cutoff;
     double space = 1.0;
     for (int d = 0; d < th.depth; d++) space *= (double)std::max(1, th.nlive);
-    st.exp_list += (double)pt.vlist.size() / space;
-    if (pt.dense) {
-      for (size_t k = 0; k + 1 < pt.voff.size(); k++)
-        st.max_list = std::max<int32_t>(st.max_list, (int32_t)(pt.voff[k + 1] - pt.voff[k]));
-    } else {
-      for (size_t k = 0; k < pt.slots.size() / 4; k++)
-        if (pt.slots[k * 4] != kHashEmpty)
-          st.max_list = std::max<int32_t>(st.max_list, (int32_t)(pt.slots[k * 4 + 3] >> 16));
-    }
+    st.exp_list += (double)pt.entries / space;
+    st.max_list = std::max<int32_t>(st.max_list, pt.max_len);
   }
   *out = st;
   return NGAP_OK;

@@ -341,12 +341,29 @@ __device__ __forceinline__ void carry_state(const MatchParams& p, WarpRun& w, in
 }
 
 // Looks up key in a prefix table: [vb, ve) of its state list when want_v and
-// [rb, re) of its report list when want_r; empty ranges when absent.
+// [rb, re) of its report list when want_r; empty ranges when absent. A
+// single-word (inline1) table gives a list of one in `one` (kNoEntry when the
+// list is empty or longer; [vb, ve) is then empty or the longer list).
 __device__ __forceinline__ void pt_find(const PrefixTableDev& t, uint32_t key, bool want_v,
                                         bool want_r, uint32_t& vb, uint32_t& ve, uint32_t& rb,
-                                        uint32_t& re) {
+                                        uint32_t& re, uint32_t& one) {
   vb = ve = rb = re = 0;
+  one = kNoEntry;
   if (!want_v && !want_r) return;
+  if (t.inline1) {  // no report lists in these tables
+    if (want_v) {
+      const uint32_t x = __ldg(t.voff + key);
+      if (x != kHashEmpty) {
+        if (x >> 31) {
+          vb = (x >> 6) & 0x1ffffffu;
+          ve = vb + (x & 63u);
+        } else {
+          one = x;
+        }
+      }
+    }
+    return;
+  }
   if (t.dense) {
     if (want_v) {
       vb = __ldg(t.voff + key);
@@ -524,10 +541,10 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
     }
   }
   const bool keep_states = k == kmax;
-  uint32_t vb = 0, ve = 0;
+  uint32_t vb = 0, ve = 0, one = kNoEntry;
   if (keep_states && k > 0) {  // one lookup: the deepest table the lane can use
     uint32_t rb, re;
-    pt_find(tv.pt[k - 1], key, true, false, vb, ve, rb, re);
+    pt_find(tv.pt[k - 1], key, true, false, vb, ve, rb, re, one);
   }
   if (tv.rep_levels) {  // reports of the first k symbols, level by level
     uint32_t kk = 0;
@@ -536,8 +553,8 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
       if (act) kk = kk * tv.nlive + c.in[r + d];
       if (!((tv.rep_levels >> d) & 1u)) continue;
       const PrefixTableDev& pt = tv.pt[d];
-      uint32_t b0, e0, rb, re;
-      pt_find(pt, kk, false, act, b0, e0, rb, re);
+      uint32_t b0, e0, rb, re, o1;
+      pt_find(pt, kk, false, act, b0, e0, rb, re, o1);
       const int len = (int)(re - rb);
       const int mx = __reduce_max_sync(kFull, len);
       for (int i = 0; i < mx; i++) {
@@ -548,7 +565,8 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
     }
   }
   // entries at the unit's last position have nothing to expand
-  const uint32_t len = (keep_states && k > 0 && q + k < c.hi) ? (ve - vb) : 0u;
+  const uint32_t len =
+      (keep_states && k > 0 && q + k < c.hi) ? (ve - vb) + (one != kNoEntry ? 1u : 0u) : 0u;
   n_injected += len;
   uint32_t incl = len;
 #pragma unroll
@@ -564,7 +582,7 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
     const uint32_t off = (uint32_t)(r + kk - 1);
     const uint32_t* vl = tv.pt[kk - 1].vlist;
     for (uint32_t j = 0; j < len; j++) {
-      const uint32_t v = __ldg(vl + vb + j);
+      const uint32_t v = one != kNoEntry ? one : __ldg(vl + vb + j);
       uint32_t e = (v << kEntryPosBits) | off;
       if (tv.sticky && is_sticky(tv, v)) {  // registered after the copy instead
         const uint32_t slot = atomicAdd(ws.pend_n, 1u);
@@ -581,8 +599,8 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
     return;
   }
   ws.inj[lane] = incl;
-  ws.inj[32 + lane] = vb;
-  ws.inj[64 + lane] = (uint32_t)(k > 0 ? k : 1);
+  ws.inj[32 + lane] = one != kNoEntry ? one : vb;  // a lone state itself, or where the list starts
+  ws.inj[64 + lane] = (uint32_t)(k > 0 ? k : 1) | (one != kNoEntry ? 0x100u : 0u);
   __syncwarp();
   // cooperative copy of all lanes' lists onto the stack
   for (uint32_t idx = lane; idx < total; idx += 32) {
@@ -593,8 +611,10 @@ __device__ __forceinline__ void inject_aas(const MatchParams& p, WarpSmem& ws, W
       else l0 = m + 1;
     }
     const uint32_t before = l0 > 0 ? ws.inj[l0 - 1] : 0u;
-    const int kk = (int)ws.inj[64 + l0];
-    const uint32_t v = __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
+    const uint32_t kraw = ws.inj[64 + l0];
+    const int kk = (int)(kraw & 0xffu);
+    const uint32_t v = (kraw & 0x100u) ? ws.inj[32 + l0]
+                                       : __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
     const uint32_t off = (uint32_t)(r0 + l0 + kk - 1);
     uint32_t e = (v << kEntryPosBits) | off;
     if (tv.sticky && is_sticky(tv, v)) {  // registered after the copy instead
@@ -625,7 +645,7 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
                                             int batch, int depth, unsigned long long& n_injected) {
   const TileDev& t = *tv.t;
   int k[2], kmax[2], r[2];
-  uint32_t key[2], vb[2], ve[2];
+  uint32_t key[2], vb[2], ve[2], one[2];
   bool valid[2];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
@@ -642,12 +662,13 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
       }
     }
     vb[h] = ve[h] = 0u;
+    one[h] = kNoEntry;
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     if (k[h] == kmax[h] && k[h] > 0) {
       uint32_t rb, re;
-      pt_find(tv.pt[k[h] - 1], key[h], true, false, vb[h], ve[h], rb, re);
+      pt_find(tv.pt[k[h] - 1], key[h], true, false, vb[h], ve[h], rb, re, one[h]);
     }
   }
   if (tv.rep_levels) {  // reports of the first k symbols, level by level
@@ -660,8 +681,8 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
         if (act) kk = kk * tv.nlive + c.in[r[h] + d];
         if (!((tv.rep_levels >> d) & 1u)) continue;
         const PrefixTableDev& pt = tv.pt[d];
-        uint32_t b0, e0, rb, re;
-        pt_find(pt, kk, false, act, b0, e0, rb, re);
+        uint32_t b0, e0, rb, re, o1;
+        pt_find(pt, kk, false, act, b0, e0, rb, re, o1);
         const int len = (int)(re - rb);
         const int mx = __reduce_max_sync(kFull, len);
         for (int i = 0; i < mx; i++) {
@@ -676,7 +697,9 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
   uint32_t len[2];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    len[h] = (k[h] == kmax[h] && k[h] > 0 && r[h] + k[h] < c.lim) ? (ve[h] - vb[h]) : 0u;
+    len[h] = (k[h] == kmax[h] && k[h] > 0 && r[h] + k[h] < c.lim)
+                 ? (ve[h] - vb[h]) + (one[h] != kNoEntry ? 1u : 0u)
+                 : 0u;
     n_injected += len[h];
   }
   const uint32_t mine = len[0] + len[1];
@@ -697,7 +720,7 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
       const uint32_t* vl = tv.pt[(k[h] > 0 ? k[h] : 1) - 1].vlist;
       for (uint32_t j = 0; j < len[h]; j++)
         store_entry(p, ws, w, w.top + (int)(pos + j),
-                    (__ldg(vl + vb[h] + j) << kEntryPosBits) | off);
+                    ((one[h] != kNoEntry ? one[h] : __ldg(vl + vb[h] + j)) << kEntryPosBits) | off);
       pos += len[h];
     }
     grow_stack(p, w, (int)total);
@@ -716,8 +739,8 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
     }
     const uint32_t ht = __shfl_sync(kFull, hi, 31);
     ws.inj[lane] = hi;
-    ws.inj[32 + lane] = vb[h];
-    ws.inj[64 + lane] = (uint32_t)(k[h] > 0 ? k[h] : 1);
+    ws.inj[32 + lane] = one[h] != kNoEntry ? one[h] : vb[h];
+    ws.inj[64 + lane] = (uint32_t)(k[h] > 0 ? k[h] : 1) | (one[h] != kNoEntry ? 0x100u : 0u);
     __syncwarp();
     for (uint32_t idx = lane; idx < ht; idx += 32) {
       int l0 = 0, l1 = 31;
@@ -727,8 +750,11 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
         else l0 = m + 1;
       }
       const uint32_t before = l0 > 0 ? ws.inj[l0 - 1] : 0u;
-      const int kk = (int)ws.inj[64 + l0];
-      const uint32_t v = __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
+      const uint32_t kraw = ws.inj[64 + l0];
+      const int kk = (int)(kraw & 0xffu);
+      const uint32_t v = (kraw & 0x100u)
+                             ? ws.inj[32 + l0]
+                             : __ldg(tv.pt[kk - 1].vlist + ws.inj[32 + l0] + (idx - before));
       const uint32_t off = (uint32_t)(r0 + 32 * h + l0 + kk - 1);
       store_entry(p, ws, w, base + (int)idx, (v << kEntryPosBits) | off);
     }

@@ -216,6 +216,26 @@ bool finish_table(PrefixTableHost& pt, uint64_t space, const Level& lv, const Ti
   while (cap < 2 * (uint64_t)nz) cap <<= 1;
   const uint64_t dense_bytes = (space + 1) * 4 * (any_rep ? 2 : 1);
   pt.dense = space <= kDenseKeys || (space <= kMaxDenseKeys && dense_bytes <= cap * 16);
+  pt.entries = (int64_t)lv.list.size();
+  for (size_t i = 0; i < nz; i++)
+    pt.max_len = std::max<int32_t>(pt.max_len, (int32_t)(lv.off[i + 1] - lv.off[i]));
+  if (pt.dense && !any_rep && pt.max_len < 64 && lv.list.size() < (1u << 25)) {
+    // one word per key: the lone state itself, or where a longer list starts
+    pt.inline1 = true;
+    pt.voff.assign(space, kHashEmpty);
+    for (size_t i = 0; i < nz; i++) {
+      const uint32_t len = lv.off[i + 1] - lv.off[i];
+      if (len == 1) {
+        pt.voff[lv.keys[i]] = lv.list[lv.off[i]];
+      } else {
+        pt.voff[lv.keys[i]] = 0x80000000u | ((uint32_t)pt.vlist.size() << 6) | len;
+        pt.vlist.insert(pt.vlist.end(), lv.list.begin() + lv.off[i], lv.list.begin() + lv.off[i + 1]);
+      }
+    }
+    pt.cutoff = nz > 0 ? (int32_t)(lv.list.size() / nz) : 0;
+    if (cutoff_opt >= 0) pt.cutoff = cutoff_opt;
+    return true;
+  }
   pt.vlist = lv.list;
   if (pt.dense) {
     pt.voff.assign(space + 1, 0);

@@ -11,11 +11,14 @@ namespace ngap {
 
 struct PrefixTableHost {
   bool dense = false;
+  bool inline1 = false;               // dense, one word per key (see PrefixTableDev::inline1)
   int32_t cutoff = 0;
   uint32_t hmask = 0;
   std::vector<uint32_t> voff, roff;   // dense
   std::vector<uint32_t> slots;        // hashed: 4 words per slot
   std::vector<uint32_t> vlist, rlist;
+  int64_t entries = 0;                // state-list entries over all keys
+  int32_t max_len = 0;                // longest state list
 };
 
 struct TileHost {

@@ -18,9 +18,14 @@ def rank_segments(num_seg, rank, world):
 
 
 def shift_offsets(reports, byte_base):
-    """Moves block-local report offsets to stream offsets."""
+    """Moves block-local report offsets (the low 32 bits) to stream offsets.
+    The reference's offsets are 32-bit (code/src/ngap/ngap.cu:1899-1905), so a
+    shifted offset past 2^32 - 1 is an error rather than a carry into the id."""
     r = np.asarray(reports, dtype=np.uint64)
-    return r + np.uint64(byte_base)
+    off = (r & np.uint64(0xFFFFFFFF)) + np.uint64(byte_base)
+    if off.size and int(off.max()) > 0xFFFFFFFF:
+        raise ValueError(f"stream offset {int(off.max())} exceeds the 32-bit report offsets")
+    return (r & ~np.uint64(0xFFFFFFFF)) | off
 
 
 def merge_reports(parts):

@@ -5,6 +5,9 @@ import os
 import socket
 
 import numpy as np
+import pytest
+
+from ngap_b200 import shard
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -79,3 +82,11 @@ def test_two_ranks_gloo(tmp_path):
     want, _ = oracle.match(groups, data, 7, 1500)
     assert len(want) > 0
     assert np.array_equal(merged, want)
+
+
+def test_shift_offsets_keeps_ids_and_refuses_overflow():
+    rep = np.array([(5 << 32) | 10, (7 << 32) | 0xFFFFFF00], dtype=np.uint64)
+    got = shard.shift_offsets(rep, 0x10)
+    assert got.tolist() == [(5 << 32) | 0x1A, (7 << 32) | 0xFFFFFF10]
+    with pytest.raises(ValueError):
+        shard.shift_offsets(rep, 0x100)  # the second offset would pass 2^32 - 1
