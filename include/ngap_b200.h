@@ -327,6 +327,12 @@ int ngap_batch_results(ngap_engine* e, uint64_t* reports, uint32_t* stream_ids, 
 int ngap_features(const uint8_t* data, uint64_t bytes, int on_device, const uint64_t* offsets,
                   const uint64_t* lengths, int n, int window, float* out, void* stream);
 
+/* The same features computed on the host, for bytes that are still in host
+ * memory (a serving loop predicting a request's work before its batch is
+ * formed): no device memory, no copy, no synchronisation. */
+int ngap_features_host(const uint8_t* data, uint64_t bytes, const uint64_t* offsets,
+                       const uint64_t* lengths, int n, int window, float* out);
+
 /* A regressor with two hidden ReLU layers of `hidden` (= 64) units and one
  * linear output; FP32 parameters on the device. */
 typedef struct ngap_mlp ngap_mlp;

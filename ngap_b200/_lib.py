@@ -156,6 +156,9 @@ SIGNATURES = {
     "ngap_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_void_p, ctypes.c_void_p]),
+    "ngap_features_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p]),
     "ngap_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "ngap_mlp_destroy": (None, [ctypes.c_void_p]),

@@ -1,6 +1,7 @@
 // Host-side C ABI: errors, ANML front-end, grouping, group views and the
 // CPU checker behind the CLI's --validation flag.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <cstdarg>
@@ -189,6 +190,55 @@ void table_find(const PrefixTableHost& t, uint32_t key, uint32_t& vb, uint32_t& 
 }
 
 }  // namespace
+
+int ngap_features_host(const uint8_t* data, uint64_t bytes, const uint64_t* offsets,
+                       const uint64_t* lengths, int n, int window, float* out) {
+  if (n < 0 || (n > 0 && (!data || !offsets || !lengths || !out)) || window < 1) {
+    set_error("ngap_features_host: bad argument");
+    return NGAP_E_INVALID;
+  }
+  for (int i = 0; i < n; i++)
+    if (offsets[i] > bytes || lengths[i] > bytes - offsets[i]) {  // no wrap-around
+      set_error("ngap_features_host: region %d is out of range", i);
+      return NGAP_E_INVALID;
+    }
+  for (int r = 0; r < n; r++) {
+    const uint8_t* p = data + offsets[r];
+    const uint64_t L = lengths[r];
+    float* o = out + (size_t)r * NGAP_FEAT_BYTES;
+    uint32_t hist[256] = {0};
+    const uint64_t W = (uint64_t)window;
+    const uint64_t nwin = L == 0 ? 0 : (L < W ? 1 : L / W);
+    const uint64_t wl = L < W ? L : W;
+    // H = log2(wl) - sum_b c_b log2(c_b) / wl, with c log2 c tabulated per window length
+    thread_local std::vector<double> clogc;
+    if (clogc.size() != wl + 1) {
+      clogc.assign(wl + 1, 0.0);
+      for (uint64_t c = 2; c <= wl; c++) clogc[c] = (double)c * std::log2((double)c);
+    }
+    const double lw = wl ? std::log2((double)wl) : 0.0;
+    double sum = 0.0, mx = 0.0;
+    for (uint64_t k = 0; k < nwin; k++) {
+      uint32_t c[256] = {0};
+      const uint8_t* q = p + k * W;
+      for (uint64_t i = 0; i < wl; i++) c[q[i]]++;
+      double s = 0.0;
+      for (int b = 0; b < 256; b++) {
+        s += clogc[c[b]];
+        hist[b] += c[b];
+      }
+      const double h = std::max(0.0, lw - s / (double)wl);
+      sum += h;
+      mx = std::max(mx, h);
+    }
+    for (uint64_t i = nwin * wl; i < L; i++) hist[p[i]]++;  // bytes past the last window
+    const double invL = L ? 1.0 / (double)L : 0.0;
+    for (int b = 0; b < 256; b++) o[b] = (float)(hist[b] * invL);
+    o[256] = nwin ? (float)(sum / (double)nwin / 8.0) : 0.f;
+    o[257] = (float)(mx / 8.0);
+  }
+  return NGAP_OK;
+}
 
 int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
                         int cap, int* n) {

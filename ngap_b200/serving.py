@@ -93,6 +93,24 @@ def host_features(data, window=cm.ENTROPY_WINDOW):
     return out
 
 
+def features_host(datas, window=cm.ENTROPY_WINDOW):
+    """host_features of several regions through the library's host
+    implementation (ngap_features_host): one call, no device work."""
+    from ._lib import check, lib
+    n = len(datas)
+    out = np.zeros((n, 258), np.float32)
+    if n == 0:
+        return out
+    lens = np.array([len(d) for d in datas], np.uint64)
+    offs = np.zeros(n, np.uint64)
+    offs[1:] = np.cumsum(lens)[:-1]
+    cat = np.ascontiguousarray(np.concatenate(datas) if lens.sum() else np.zeros(1, np.uint8),
+                               dtype=np.uint8)
+    check(lib().ngap_features_host(cat.ctypes.data, int(lens.sum()), offs.ctypes.data,
+                                   lens.ctypes.data, n, int(window), out.ctypes.data))
+    return out
+
+
 def host_features_many(datas, window=cm.ENTROPY_WINDOW):
     """host_features of several regions; row i equals host_features(datas[i]).
     Regions of one common length that is a multiple of `window` (full 16 KiB
@@ -142,7 +160,7 @@ class Predictor:
         nf = np.array([r.nfa for r in reqs], dtype=np.int64)
         if self.kind != "learned":
             return self.static.predict(nf)
-        feats = host_features_many([r.data[:cm.REGION] for r in reqs])
+        feats = features_host([r.data[:cm.REGION] for r in reqs])
         x = np.concatenate([feats, self.nfeat[nf]], axis=1).astype(np.float32)
         return self.model.predict(nf, x, bf16=True)
 

@@ -57,6 +57,31 @@ def test_host_features_definition():
         assert np.isclose(f[257], np.max(hs) / 8, atol=1e-6)
 
 
+def test_library_host_features_agree(built):
+    """ngap_features_host (the library's C implementation the serving loop
+    predicts with) against host_features, including empty, sub-window and
+    ragged regions, and its argument checks."""
+    from ngap_b200._lib import lib
+    rng = np.random.default_rng(3)
+    datas = [rng.integers(0, 256 if i % 2 else 5, size=L).astype(np.uint8)
+             for i, L in enumerate((0, 1, 500, 1023, 1024, 1025, 3000, 16384, 16385))]
+    datas.append(np.zeros(4096, np.uint8))
+    got = sv.features_host(datas)
+    want = np.stack([sv.host_features(d) for d in datas])
+    assert np.allclose(got, want, rtol=0, atol=1e-6)
+    assert sv.features_host([]).shape == (0, 258)
+    d = np.zeros(16, np.uint8)
+    off = np.array([8], np.uint64)
+    ln = np.array([9], np.uint64)  # 8 + 9 > 16
+    out = np.zeros(258, np.float32)
+    rc = lib().ngap_features_host(d.ctypes.data, 16, off.ctypes.data, ln.ctypes.data, 1, 1024,
+                                  out.ctypes.data)
+    assert rc != 0
+    rc = lib().ngap_features_host(d.ctypes.data, 16, off.ctypes.data, ln.ctypes.data, 1, 0,
+                                  out.ctypes.data)
+    assert rc != 0
+
+
 def test_poisson_requests():
     rng = np.random.default_rng(1)
     pool = [rng.integers(0, 256, 4096, dtype=np.uint8) for _ in range(6)]
