@@ -140,6 +140,9 @@ typedef struct ngap_tile_desc {
   int32_t max_path;   /* longest acyclic path (chunk warm-up + 1); -1 = cyclic */
   int32_t nlive;      /* live byte classes */
   int32_t dense_levels; /* bit d-1 set: table d is dense (offsets by key), else hashed */
+  int32_t naas;       /* always-active states in the tile */
+  int32_t shortcuts;  /* layered tiles: successors their sticky states enable from their
+                         first match on (edges of the CC's states into them dropped) */
   int64_t table_bytes; /* prefix tables and image */
 } ngap_tile_desc;
 int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_tile_desc* out,
@@ -237,13 +240,14 @@ int ngap_engine_test_wait_timeout(ngap_engine* e, int32_t unit, int32_t wait_rou
 /* Generalises --motivate-worklist-length (code/src/ngap/kernel_ngap_OA.cu:366-369,
  * code/src/ngap/ngap.cu:1843-1866), which records the fetched worklist length
  * per round: with tracing on, every later match (plain or batched) records
- * the worklist work of each unit (one tile over one chunk of a segment or
- * stream). */
+ * the worklist work and the duration of each unit (one tile over one chunk
+ * of a segment or stream). */
 typedef struct ngap_unit_trace {
   int32_t stream;   /* segment (ngap_match) or stream (ngap_batch_match) index */
   int32_t tile;     /* tile index (in the tableset for batched matches) */
   int64_t lo, hi;   /* positions whose reports the unit owns, relative to its segment/stream */
   uint64_t work;    /* worklist entries the unit expanded plus entries it injected */
+  uint64_t cycles;  /* SM clock cycles from the unit's start to its end (one warp) */
 } ngap_unit_trace;
 int ngap_engine_set_trace(ngap_engine* e, int enable);
 /* Copies up to cap of the last match's unit records (after ngap_engine_sync);

@@ -59,7 +59,8 @@ class TableOpts(ctypes.Structure):
 class TileDesc(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in (
         "phase", "pair", "group", "num_states", "num_ccs", "nact", "nsticky", "global_",
-        "depth", "max_path", "nlive", "dense_levels")] + [("table_bytes", ctypes.c_int64)]
+        "depth", "max_path", "nlive", "dense_levels", "naas", "shortcuts")] + \
+        [("table_bytes", ctypes.c_int64)]
 
 
 class MatchParams(ctypes.Structure):
@@ -90,7 +91,7 @@ class EngineMem(ctypes.Structure):
 
 class UnitTrace(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_int32), ("tile", ctypes.c_int32), ("lo", ctypes.c_int64),
-                ("hi", ctypes.c_int64), ("work", ctypes.c_uint64)]
+                ("hi", ctypes.c_int64), ("work", ctypes.c_uint64), ("cycles", ctypes.c_uint64)]
 
 
 class TablesStats(ctypes.Structure):

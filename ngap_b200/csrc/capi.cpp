@@ -265,6 +265,8 @@ int ngap_tiles_describe(const ngap_groups* g, const ngap_table_opts* opts, ngap_
     d.depth = t.depth;
     d.max_path = t.max_path;
     d.nlive = t.nlive;
+    d.naas = (int32_t)t.aas.size();
+    for (uint32_t a : t.act_local) d.shortcuts += __builtin_popcount(a >> 28);
     int64_t b = (int64_t)t.image.size();
     for (int k = 0; k < t.depth; k++) {
       const PrefixTableHost& p = t.pt[k];

@@ -8,6 +8,10 @@
 namespace ngap {
 
 constexpr uint32_t kNoSucc = 0xffffffffu;
+// act_local of layered tiles: local id of the slot's sticky state in the low
+// 28 bits; bit 28 + j set when the state enables its successor j from its
+// first match on (a shortcut) rather than from the next position
+constexpr uint32_t kActIdMask = 0x0fffffffu;
 constexpr int kMaxDepth = 12;        // prefix-memoization depth limit (the reference stops at 3)
 constexpr int kEntryPosBits = 13;    // worklist entry = local_state << 13 | window offset
 constexpr int kMaxWindow = (1 << kEntryPosBits) - 2;
@@ -81,7 +85,7 @@ struct TileDev {
   int32_t off_sticky = 0;
   int32_t phase = 0;        // 0 plain; 1 activation pass; 2 layered (sticky states pre-registered)
   int32_t nact = 0;         // activation slots per segment (phase 1 and 2)
-  const uint32_t* act_local = nullptr;  // phase 2: [nact] local id of each slot's sticky state
+  const uint32_t* act_local = nullptr;  // phase 2: [nact] each slot's sticky state (kActIdMask)
   const uint32_t* stk_union = nullptr;  // phase 2: [nact][cw] classes any successor accepts
   const uint8_t* image = nullptr;   // global copy of the image (16-byte aligned)
   const uint32_t* sid = nullptr;    // [nstates] local -> report id (sid | group << 22)

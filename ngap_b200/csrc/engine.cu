@@ -608,19 +608,22 @@ ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
 }
 
 // Per-unit work counters when tracing (zeroed on st); null otherwise.
-int trace_buffer(ngap_engine* e, cudaStream_t st, unsigned long long** out) {
-  *out = nullptr;
+// d_unit_work holds two arrays of unit_work_cap words: work, then cycles
+int trace_buffer(ngap_engine* e, cudaStream_t st, unsigned long long** work,
+                 unsigned long long** cycles) {
+  *work = *cycles = nullptr;
   if (!e->trace || e->nunits == 0) return NGAP_OK;
   if ((size_t)e->nunits > e->unit_work_cap) {
     const size_t cap = grown(e->unit_work_cap, (size_t)e->nunits);
     cudaFree(e->d_unit_work);
     e->d_unit_work = nullptr;
     e->unit_work_cap = 0;
-    CUDA_TRY(cudaMalloc(&e->d_unit_work, cap * sizeof(unsigned long long)));
+    CUDA_TRY(cudaMalloc(&e->d_unit_work, 2 * cap * sizeof(unsigned long long)));
     e->unit_work_cap = cap;
   }
   CUDA_TRY(cudaMemsetAsync(e->d_unit_work, 0, (size_t)e->nunits * sizeof(unsigned long long), st));
-  *out = e->d_unit_work;
+  *work = e->d_unit_work;
+  *cycles = e->d_unit_work + e->unit_work_cap;
   return NGAP_OK;
 }
 
@@ -1155,7 +1158,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   mp.skip_copy_unit = e->test_skip_unit;
   e->test_wait_rounds = 0;  // the hook covers one match
   e->test_skip_unit = -1;
-  if ((rc = trace_buffer(e, st, &mp.unit_work)) != NGAP_OK) return rc;
+  if ((rc = trace_buffer(e, st, &mp.unit_work, &mp.unit_cycles)) != NGAP_OK) return rc;
   e->trace_seg_len = p->seg_len;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
   if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0) {
@@ -1256,7 +1259,7 @@ int ngap_engine_memory(const ngap_engine* e, ngap_engine_mem* out) {
   out->reports = 3 * 8 * (int64_t)e->rep_cap + 4 * (int64_t)e->hist_cap + 4 * (int64_t)e->stream_ids_cap;
   out->scratch =
       (int64_t)e->slots * 4 * ((int64_t)e->carry_cap + e->mark_words + e->ovf_cap + 2 * e->stk_cap);
-  out->plan = 8 * (int64_t)e->act_cap + 16 * (int64_t)e->rows_cap + 8 * (int64_t)e->unit_work_cap +
+  out->plan = 8 * (int64_t)e->act_cap + 16 * (int64_t)e->rows_cap + 16 * (int64_t)e->unit_work_cap +
               (int64_t)sizeof(UnitDev) * (int64_t)e->units_cap +
               (int64_t)sizeof(TaskDev) * (int64_t)e->tasks_cap;
   return NGAP_OK;
@@ -1298,11 +1301,13 @@ int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* 
     *n = e->nunits;
     return NGAP_OK;
   }
-  std::vector<unsigned long long> work(e->nunits);
+  std::vector<unsigned long long> work(e->nunits), cycles(e->nunits);
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   CUDA_TRY(cudaMemcpy(work.data(), e->d_unit_work, work.size() * sizeof(unsigned long long),
                       cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(cycles.data(), e->d_unit_work + e->unit_work_cap,
+                      cycles.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   const int64_t m = std::min<int64_t>(cap, e->nunits);
   for (int64_t i = 0; i < m; i++) {
     const UnitDev& u = e->h_units[i];
@@ -1312,6 +1317,7 @@ int ngap_trace_copy(ngap_engine* e, ngap_unit_trace* out, int64_t cap, int64_t* 
     out[i].lo = u.emit_lo - base;
     out[i].hi = u.hi - base;
     out[i].work = work[i];
+    out[i].cycles = cycles[i];
   }
   *n = m;
   return NGAP_OK;
@@ -1599,14 +1605,14 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   mp.act_cnt = e->d_act_cnt;
   mp.stk_g = e->d_stk;
   mp.stk_g_cap = e->stk_cap;
-  mp.unit_work = nullptr;
+  mp.unit_work = mp.unit_cycles = nullptr;
   mp.wait_rounds = kWaitRounds;
   mp.skip_copy_unit = -1;
   e->trace_seg_len = 0;
 
   auto enqueue = [&](cudaStream_t qs) -> int {
     if (e->trace) {
-      const int r = trace_buffer(e, qs, &mp.unit_work);
+      const int r = trace_buffer(e, qs, &mp.unit_work, &mp.unit_cycles);
       if (r != NGAP_OK) return r;
     }
     if (input_on_device)

@@ -83,6 +83,7 @@ struct MatchParams {
   uint32_t* stk_g;          // [slots][2][stk_g_cap]: sticky lists of layered units beyond
   int32_t stk_g_cap;        // kStickyCap
   unsigned long long* unit_work;  // [units]: entries expanded + injected per unit (tracing), or null
+  unsigned long long* unit_cycles;  // [units]: SM clock cycles per unit (tracing), or null
   int32_t free_begin;       // units [free_begin, free_begin + nfree) are taken warp by warp
   int32_t nfree;
   int32_t free_tile;        // the one tile of all free units (descriptors staged per CTA), or -1
@@ -635,41 +636,104 @@ __device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem&
                                                  const TileView& tv, const UnitCtx& c, int lane,
                                                  int r0, int batch);
 
+// Table words of the next injection batch, read ahead (see inject_aas2):
+// kf[h] = k | use << 8 | word << 9 for the lane's position h (use: the whole
+// key is live and the list is wanted; word: x[h] holds its inline1 word).
+struct InjAhead {
+  int r0 = -1 << 30;  // window offset of the batch they belong to; invalid otherwise
+  uint32_t x[2];
+  uint32_t kf[2];
+};
+
+// The lane's position h of the batch at r0: k (live classes of the next
+// symbols, a dead class or the window end stop it), whether the whole key is
+// live (use), and the key.
+__device__ __forceinline__ void inject_key(const TileView& tv, const UnitCtx& c, int lane, int r0,
+                                           int batch, int depth, int h, int& k, bool& use,
+                                           uint32_t& key) {
+  const int r = r0 + 32 * h + lane;
+  const bool valid = 32 * h + lane < batch && r < c.iend;
+  const int kmax = valid ? min(depth, c.wlen - r) : 0;
+  k = kmax;
+  key = 0u;
+  for (int d = 0; d < depth; d++) {
+    if (d < k) {
+      const uint32_t sym = c.in[r + d];
+      if (sym >= tv.nlive) k = d;
+      else key = key * tv.nlive + sym;
+    }
+  }
+  use = k == kmax && k > 0;
+}
+
 // Always-active states through the prefix tables for window offsets
 // [r0, r0 + batch), batch <= 64, two positions per lane (r0 + lane and
 // r0 + 32 + lane), for tiles without sticky states: both table lookups of a
 // lane are issued before either list is read, so a warp has two lookups in
 // flight per lane. Same entries and reports as inject_aas over the two halves.
+// AHEAD (the lean PRIV 0 instances): after this batch's lookups, the lane's inline
+// table words of the next batch are read too, and the next call uses them.
+template <bool AHEAD>
 __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, WarpRun& w,
                                             const TileView& tv, const UnitCtx& c, int lane, int r0,
-                                            int batch, int depth, unsigned long long& n_injected) {
+                                            int batch, int depth, unsigned long long& n_injected,
+                                            InjAhead& ahead) {
   const TileDev& t = *tv.t;
-  int k[2], kmax[2], r[2];
-  uint32_t key[2], vb[2], ve[2], one[2];
-  bool valid[2];
+  int k[2], r[2];
+  bool use[2];
+  uint32_t vb[2], ve[2], one[2];
+  const bool read_ahead = AHEAD && ahead.r0 == r0;  // read during the last batch's expansions
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     r[h] = r0 + 32 * h + lane;
-    valid[h] = 32 * h + lane < batch && r[h] < c.iend;
-    kmax[h] = valid[h] ? min(depth, c.wlen - r[h]) : 0;
-    k[h] = kmax[h];
-    key[h] = 0u;
-    for (int d = 0; d < depth; d++) {
-      if (d < k[h]) {
-        const uint32_t sym = c.in[r[h] + d];
-        if (sym >= tv.nlive) k[h] = d;
-        else key[h] = key[h] * tv.nlive + sym;
-      }
-    }
     vb[h] = ve[h] = 0u;
     one[h] = kNoEntry;
-  }
-#pragma unroll
-  for (int h = 0; h < 2; h++) {
-    if (k[h] == kmax[h] && k[h] > 0) {
-      uint32_t rb, re;
-      pt_find(tv.pt[k[h] - 1], key[h], true, false, vb[h], ve[h], rb, re, one[h]);
+    uint32_t key = 0u;
+    bool word = false;
+    if (read_ahead) {
+      k[h] = (int)(ahead.kf[h] & 0xffu);
+      use[h] = (ahead.kf[h] >> 8) & 1u;
+      word = (ahead.kf[h] >> 9) & 1u;
     }
+    if (!read_ahead || (use[h] && !word)) inject_key(tv, c, lane, r0, batch, depth, h, k[h], use[h], key);
+    if (!use[h]) continue;
+    if (word) {  // decode the inline1 word read ahead
+      const uint32_t x = ahead.x[h];
+      if (x != kHashEmpty) {
+        if (x >> 31) {
+          vb[h] = (x >> 6) & 0x1ffffffu;
+          ve[h] = vb[h] + (x & 63u);
+        } else {
+          one[h] = x;
+        }
+      }
+    } else {
+      uint32_t rb, re;
+      pt_find(tv.pt[k[h] - 1], key, true, false, vb[h], ve[h], rb, re, one[h]);
+    }
+  }
+  // read the next batch's table words now: their DRAM round trip overlaps
+  // this batch's list copies and the expansions that follow
+  ahead.r0 = -1 << 30;
+  const int r1 = r0 + batch;
+  if (AHEAD && r1 < c.iend) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      int kn;
+      bool un;
+      uint32_t key;
+      inject_key(tv, c, lane, r1, batch, depth, h, kn, un, key);
+      bool word = false;
+      if (un) {
+        const PrefixTableDev& pt = tv.pt[kn - 1];
+        if (pt.inline1) {
+          ahead.x[h] = __ldg(pt.voff + key);
+          word = true;
+        }
+      }
+      ahead.kf[h] = (uint32_t)kn | (un ? 0x100u : 0u) | (word ? 0x200u : 0u);
+    }
+    ahead.r0 = r1;
   }
   if (tv.rep_levels) {  // reports of the first k symbols, level by level
 #pragma unroll
@@ -697,7 +761,7 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
   uint32_t len[2];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    len[h] = (k[h] == kmax[h] && k[h] > 0 && r[h] + k[h] < c.lim)
+    len[h] = (use[h] && r[h] + k[h] < c.lim)
                  ? (ve[h] - vb[h]) + (one[h] != kNoEntry ? 1u : 0u)
                  : 0u;
     n_injected += len[h];
@@ -878,36 +942,45 @@ __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, W
   const bool emit = valid && tp >= c.emit_lo;
   if (w.stk_rep) {  // a reporting sticky state reports at every position after its first match
     for (int i = 0; i < w.nstk; i++) {
-      const uint32_t s = __ldg(t.act_local + ws.stk_s[i]);
+      const uint32_t s = __ldg(t.act_local + ws.stk_s[i]) & kActIdMask;
       const bool rs = emit && tp > (int64_t)ws.stk_q[i] && is_report(tv, s);
       emit_report(p, ws, w, lane, rs, rs ? __ldg(t.sid + s) : 0u, (uint32_t)tp);
     }
   }
+  // successors of slot i enabled at tp: all of them after its first match,
+  // the shortcut ones (act_local bits 28..31) at it
+  auto enabled = [&](int i, uint32_t al) -> uint32_t {
+    const int64_t q = (int64_t)ws.stk_q[i];
+    return !valid || tp < q ? 0u : (tp > q ? 0xfu : al >> 28);
+  };
   const uint32_t word = sym >> 5, bit = 1u << (sym & 31);
   int cnt = 0;
   bool any_rep = false;
   for (int i = 0; i < w.nstk; i++) {
-    if (!(valid && tp > (int64_t)ws.stk_q[i])) continue;
+    if (!(valid && tp >= (int64_t)ws.stk_q[i])) continue;
     const uint32_t slot = ws.stk_s[i];
     if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
-    const uint4 sc = load_succ(tv, __ldg(t.act_local + slot));
+    const uint32_t al = __ldg(t.act_local + slot);
+    const uint32_t on = enabled(i, al);
+    const uint4 sc = load_succ(tv, al & kActIdMask);
     const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
 #pragma unroll
     for (int j = 0; j < 4; j++)
-      if (us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym)) {
+      if (((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym)) {
         cnt++;
         any_rep |= (us[j] >> 31) && emit;
       }
   }
   if (__any_sync(kFull, any_rep)) {
     for (int i = 0; i < w.nstk; i++) {
-      const bool act = valid && tp > (int64_t)ws.stk_q[i];
-      const uint4 sc = load_succ(tv, __ldg(t.act_local + ws.stk_s[i]));
+      const uint32_t al = __ldg(t.act_local + ws.stk_s[i]);
+      const uint32_t on = enabled(i, al);
+      const uint4 sc = load_succ(tv, al & kActIdMask);
       const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
       bool ok[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        ok[j] = act && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
+        ok[j] = ((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
       report4(p, ws, w, tv, lane, ok, us, tp, emit);
     }
   }
@@ -923,15 +996,17 @@ __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, W
   if (pc) {
     int pos = w.top + incl - pc;
     for (int i = 0; i < w.nstk; i++) {
-      if (tp <= (int64_t)ws.stk_q[i]) continue;
+      if (tp < (int64_t)ws.stk_q[i]) continue;
       const uint32_t slot = ws.stk_s[i];
       if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
-      const uint4 sc = load_succ(tv, __ldg(t.act_local + slot));
+      const uint32_t al = __ldg(t.act_local + slot);
+      const uint32_t on = enabled(i, al);
+      const uint4 sc = load_succ(tv, al & kActIdMask);
       const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const uint32_t u = us[j] & kIdMask;
-        if (us[j] != kNoSucc && accepts(tv, u, sym))
+        if (((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, u, sym))
           store_entry(p, ws, w, pos++, (u << kEntryPosBits) | (uint32_t)r);
       }
     }
@@ -1196,7 +1271,7 @@ __device__ __forceinline__ void tile_run(const MatchParams& p, const TileDev* t,
   tv.nlive = (uint32_t)t->nlive;
   tv.rep_levels = 0u;
   for (int d = 0; d < kMaxDepth; d++) tv.rep_levels |= (pt[d].has_reports ? 1u : 0u) << d;
-  tr.depth = p.depth == 0 ? 0 : min(p.depth, t->depth);
+  tr.depth = p.depth == 0 || t->naas == 0 ? 0 : min(p.depth, t->depth);
   tr.batch = tr.depth == 0 ? t->inj_batch0 : t->inj_batch;
   // short table lists, no sticky states: two positions per lane per injection
   tr.wide_inject = tr.depth > 0 && !tv.sticky && tr.batch == 32;
@@ -1283,10 +1358,11 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     return bytes;
   };
 
-  // sticky list of the tile: shared memory, or global memory for layered
-  // tiles with more slots than that holds
-  auto sticky_lists = [&](const TileDev* t, bool layered) {
-    if (layered && t->nact > kStickyCap && p.stk_g_cap >= t->nact) {
+  // sticky list of a unit: shared memory, or global memory for layered units
+  // with more activations (n) than that holds. (Global stores are not
+  // cached in L1: a list there costs an L2 round trip per read.)
+  auto sticky_lists = [&](const TileDev* t, bool layered, uint32_t n) {
+    if (layered && n > (uint32_t)kStickyCap && p.stk_g_cap >= t->nact) {
       ws.stk_s = p.stk_g + (size_t)slot * 2 * p.stk_g_cap;
       ws.stk_q = ws.stk_s + p.stk_g_cap;
       w.stk_cap = p.stk_g_cap;
@@ -1304,6 +1380,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
     const bool layered = tr.layered, wide_inject = tr.wide_inject;
     const UnitDev un = p.units[uid];
     const unsigned long long work0 = n_expanded + n_injected;  // per-unit trace
+    if (p.unit_work && lane == 0) p.unit_cycles[uid] = clock64();  // start; the end subtracts
     UnitCtx c;
     c.hi = un.hi;
     c.emit_lo = un.emit_lo;
@@ -1317,6 +1394,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       // unit's end: active from there on; a reporting one also reports at
       // its first match
       const uint32_t n = p.act_cnt[un.act_rowid];
+      sticky_lists(t, true, n);
       bool rep_any = false;
       for (uint32_t i0 = 0; i0 < n; i0 += 32) {
         const uint32_t i = i0 + lane;
@@ -1325,7 +1403,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         const int64_t q = un.base + (int64_t)f;
         const bool ok = f != kNoAct && q < c.hi;
         const unsigned m = __ballot_sync(kFull, ok);
-        const uint32_t sv = ok ? __ldg(t->act_local + sl) : 0u;
+        const uint32_t sv = ok ? __ldg(t->act_local + sl) & kActIdMask : 0u;
         if (ok) {
           const int k = w.nstk + __popc(m & lanemask_lt(lane));
           if (k < w.stk_cap) {
@@ -1344,11 +1422,16 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       w.stk_rep = __any_sync(kFull, rep_any);
       __syncwarp();
     }
+    // nothing can become active in a layered unit without sticky states,
+    // always-active states or start-of-data states at its first position
+    // (such a unit runs no window: its end is moved to its start)
+    if (layered && w.nstk == 0 && t->naas == 0 && !((un.flags & 1u) && t->nstart > 0))
+      c.hi = un.lo;
     int cur = 0;
     uint32_t nbytes[2], skip[2];
-    if ((int32_t)uid != p.skip_copy_unit) {
+    if (c.hi > un.lo && (int32_t)uid != p.skip_copy_unit) {
       nbytes[0] = issue(0, un.lo, c.hi, 0, skip[0]);
-    } else {  // test hook: nothing is in flight, the first wait gives up
+    } else {  // idle, or the test hook: nothing is in flight (the hook's first wait gives up)
       nbytes[0] = 0u;
       skip[0] = 0u;
     }
@@ -1406,7 +1489,10 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       }
       // next window offset to inject: negative for positions deferred from
       // the previous window (at most `defer` of them)
-      int cursor = (int)(inj_pos - wb);
+      // (without always-active states only plain sticky tiles have injection
+      // work: their registered sticky states, batch by batch)
+      int cursor = t->naas == 0 && (LEAN || layered || !tv.sticky) ? c.iend : (int)(inj_pos - wb);
+      InjAhead ahead;  // table words of the next batch, read ahead (this window only)
       // layered tiles: next window offset of the sticky states' work
       int scur = layered && w.nstk > 0 ? 0 : c.wlen;
       while (true) {
@@ -1415,7 +1501,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
         if (w.top < kInjectLow && w.ovf_n == 0) {
           if (cursor < c.iend) {
             if (wide_inject) {
-              inject_aas2(p, ws, w, tv, c, lane, cursor, 2 * batch, depth, n_injected);
+              inject_aas2<LEAN && PRIV == 0>(p, ws, w, tv, c, lane, cursor, 2 * batch, depth,
+                                             n_injected, ahead);
               cursor += 2 * batch;
             } else if (LEAN) {
               inject_aas(p, ws, w, tv, c, lane, cursor, batch, depth, n_injected);
@@ -1460,7 +1547,10 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       unsigned long long d = n_expanded + n_injected - work0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
-      if (lane == 0) p.unit_work[uid] = d;
+      if (lane == 0) {
+        p.unit_work[uid] = d;
+        p.unit_cycles[uid] = clock64() - p.unit_cycles[uid];
+      }
     }
     if (dead) {
       for (int i = lane; i < w.ncarry; i += 32) w.marks[w.carry[i] >> 5] = 0u;
@@ -1566,7 +1656,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       tile_run<LEAN>(p, t, t->image, s_pt, s_cls, tr);
     else
       tile_run<LEAN>(p, t, t->image, t->pt, t->image + t->off_cls, tr);
-    sticky_lists(t, tr.layered);
+    sticky_lists(t, false, 0u);  // layered units choose theirs by their activation count
     run_unit(uid, t, tr);
   }
   flush_reports(p, ws, w, lane);

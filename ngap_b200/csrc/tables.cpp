@@ -138,6 +138,80 @@ bool layer_flags(const GroupGraph& g, int32_t b, int32_t e, std::vector<char>& s
   return true;
 }
 
+// Shortcuts through the sticky states of a layered CC, for its layered tile.
+// For a sticky state s that is not a start-of-data state, let P be the
+// states with an edge into s (other than its self-loop) and D the successors
+// u of s (not s, not always-active, not sticky) that every state of P also
+// leads to. When v in P matches at q, s matches at q + 1 (it accepts every
+// byte), so s's first match f is at most q + 1: v's edge enables u at q + 1,
+// which s enables as well when q + 1 > f; and at q + 1 = f, s was enabled by
+// some state of P (s is no start state), whose edge enables u at f. So the
+// edges P -> D can go if s enables D from its first match on (inclusive)
+// instead of after it. States that then reach no report state through the
+// remaining edges (edges into always-active or sticky states do not count)
+// are left out of the layered tile; sticky states stay (activation slots).
+// drop[k - row_offsets[b]] marks dropped edges, dset[s - b] lists D of s,
+// keep[v - b] the states of the layered tile.
+void layered_shortcuts(const GroupGraph& g, int32_t b, int32_t e, const std::vector<char>& sticky,
+                       std::vector<char>& drop, std::vector<std::vector<int32_t>>& dset,
+                       std::vector<char>& keep) {
+  const int32_t n = e - b, e0 = g.row_offsets[b];
+  drop.assign(g.row_offsets[e] - e0, 0);
+  dset.assign(n, {});
+  std::vector<std::vector<int32_t>> pred(n);
+  for (int32_t v = b; v < e; v++)
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (u != v && sticky[u - b]) pred[u - b].push_back(v);
+    }
+  auto has_edge = [&](int32_t v, int32_t u) {
+    return std::binary_search(g.cols.begin() + g.row_offsets[v],
+                              g.cols.begin() + g.row_offsets[v + 1], u);  // rows are sorted
+  };
+  for (int32_t s = b; s < e; s++) {
+    if (!sticky[s - b] || pred[s - b].empty() ||
+        std::binary_search(g.starts.begin(), g.starts.end(), s))
+      continue;
+    std::vector<int32_t>& d = dset[s - b];
+    for (int32_t k = g.row_offsets[s]; k < g.row_offsets[s + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if (u == s || (g.attrs[u] & 1) || sticky[u - b]) continue;
+      bool all = true;
+      for (int32_t v : pred[s - b]) all = all && has_edge(v, u);
+      if (all) d.push_back(u);
+    }
+    for (int32_t v : pred[s - b])
+      for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++)
+        if (std::binary_search(d.begin(), d.end(), g.cols[k])) drop[k - e0] = 1;
+  }
+  // states that reach a report state through the kept edges (reverse search)
+  std::vector<std::vector<int32_t>> rev(n);
+  for (int32_t v = b; v < e; v++)
+    for (int32_t k = g.row_offsets[v]; k < g.row_offsets[v + 1]; k++) {
+      const int32_t u = g.cols[k];
+      if ((g.attrs[u] & 1) || sticky[u - b] || drop[k - e0]) continue;
+      rev[u - b].push_back(v);
+    }
+  keep.assign(n, 0);
+  std::vector<int32_t> todo;
+  for (int32_t v = b; v < e; v++)
+    if (g.attrs[v] & 2) {
+      keep[v - b] = 1;
+      todo.push_back(v);
+    }
+  while (!todo.empty()) {
+    const int32_t u = todo.back();
+    todo.pop_back();
+    for (int32_t v : rev[u - b])
+      if (!keep[v - b]) {
+        keep[v - b] = 1;
+        todo.push_back(v);
+      }
+  }
+  for (int32_t i = 0; i < n; i++)
+    if (sticky[i]) keep[i] = 1;
+}
+
 // Longest path (in states) of a CC whose edges into always-active states are
 // removed; -1 if a cycle remains.
 int32_t cc_longest_path(const GroupGraph& g, int32_t b, int32_t e) {
@@ -456,6 +530,9 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
   // per CC: local ids of its states in the tile (-1: not in the tile) and sticky flags
   std::vector<std::vector<int32_t>> loc(ccs.size());
   std::vector<std::vector<char>> stk(ccs.size());
+  // layered tiles: dropped edges, shortcut successors of each sticky state, kept states
+  std::vector<std::vector<char>> drop(ccs.size()), keep(ccs.size());
+  std::vector<std::vector<std::vector<int32_t>>> dset(ccs.size());
   int32_t n = 0;
   bool bounded = true;
   int32_t mp = 0;
@@ -468,6 +545,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
     if (variant != kPlain) {
       if (!layer_flags(g, c.begin, c.end, stk[ci], pre, lp1, lp2)) return false;
       mp = std::max(mp, variant == kActivation ? lp1 : lp2);
+      if (variant == kLayered) layered_shortcuts(g, c.begin, c.end, stk[ci], drop[ci], dset[ci], keep[ci]);
     } else {
       bounded = bounded && c.bounded;
       mp = std::max(mp, c.max_path);
@@ -475,6 +553,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
     loc[ci].assign(c.end - c.begin, -1);
     for (int32_t v = c.begin; v < c.end; v++) {
       if (variant == kActivation && !pre[v - c.begin]) continue;
+      if (variant == kLayered && !keep[ci][v - c.begin]) continue;
       loc[ci][v - c.begin] = n++;
       part.refine(&g.bits[(size_t)v * 8]);
     }
@@ -517,6 +596,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
   t.sid.resize(n);
   std::vector<uint32_t> aas_bit((n + 31) / 32, 0);
   t.sticky.assign((n + 31) / 32, 0);
+  std::vector<int32_t> act_cc;  // layered tiles: CC of each activation slot
   for (size_t ci = 0; ci < ccs.size(); ci++) {
     const CcInfo& c = ccs[ci];
     const GroupGraph& g = gs.groups[c.group];
@@ -545,6 +625,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
       if (variant == kLayered && sv) {
         t.sticky[local >> 5] |= 1u << (local & 31);
         t.act_local.push_back((uint32_t)local);
+        act_cc.push_back((int32_t)ci);
         t.nact++;
       }
       if (g.attrs[v] & 1) {
@@ -560,6 +641,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
           // into a sticky state: kept only by the activation part (not its self-loop)
           if (variant == kLayered || u == v) continue;
         }
+        if (variant == kLayered && drop[ci][k - g.row_offsets[c.begin]]) continue;  // a shortcut
         const int32_t ul = lc[u - c.begin];
         if (ul < 0) continue;          // not a pre state: no path to a sticky state
         if (j >= 4) return false;      // the degree limiter guarantees at most 4
@@ -572,6 +654,25 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
     auto lo = std::lower_bound(g.starts.begin(), g.starts.end(), c.begin);
     for (auto it = lo; it != g.starts.end() && *it < c.end; ++it)
       if (lc[*it - c.begin] >= 0) t.start.push_back((uint32_t)lc[*it - c.begin]);
+  }
+  // layered tiles: bits 28..31 of a slot's act_local mark its successors
+  // (record order) that the sticky state enables from its first match on
+  // (shortcuts, layered_shortcuts); the others it enables after it
+  if (variant == kLayered) {
+    if (n > (int32_t)kActIdMask) return false;
+    for (int32_t i = 0; i < t.nact; i++) {
+      const CcInfo& c = ccs[act_cc[i]];
+      const uint32_t s = t.act_local[i];
+      const std::vector<int32_t>& d = dset[act_cc[i]][(t.sid[s] & 0x3fffffu) - c.begin];
+      uint32_t incl = 0;
+      for (int j = 0; j < 4; j++) {
+        const uint32_t u = t.succ[(size_t)s * 4 + j];
+        if (u != kNoSucc &&
+            std::binary_search(d.begin(), d.end(), (int32_t)(t.sid[u & 0x7fffffffu] & 0x3fffffu)))
+          incl |= 1u << j;
+      }
+      t.act_local[i] = s | incl << 28;
+    }
   }
   // sticky states of plain tiles: not always-active, a self-loop and every
   // byte accepted; once such a state matches it matches at every later
@@ -592,7 +693,7 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
   if (variant == kLayered) {  // union of the successors' class masks of every slot
     t.stk_union.assign((size_t)t.nact * t.cw, 0);
     for (int32_t i = 0; i < t.nact; i++) {
-      const uint32_t s = t.act_local[i];
+      const uint32_t s = t.act_local[i] & kActIdMask;
       for (int j = 0; j < 4; j++) {
         const uint32_t u = t.succ[(size_t)s * 4 + j];
         if (u == kNoSucc) continue;

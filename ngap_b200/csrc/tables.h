@@ -37,7 +37,7 @@ struct TileHost {
   int32_t phase = 0;                 // 0 plain, 1 activation pass, 2 layered (stickies from pass 1)
   int32_t pair = -1;                 // activation/layered tiles: index of their pair
   int32_t nact = 0;                  // activation slots (sticky states) of the pair
-  std::vector<uint32_t> act_local;   // layered: local id of the sticky state of each slot
+  std::vector<uint32_t> act_local;   // layered: sticky state of each slot and its shortcut bits (kActIdMask)
   std::vector<uint32_t> stk_union;   // layered: [nact][cw] classes any successor of the slot accepts
   std::vector<uint8_t> cls;          // 256: byte -> class, live classes first
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor

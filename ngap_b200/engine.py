@@ -143,7 +143,8 @@ class Groups:
     def tiles(self, precompute_depth=0, tile_states=0, tile_mode="auto", max_table_entries=0):
         """The tiles Tables(...) would build, planned on the host (no GPU):
         list of dicts (phase, pair, group, num_states, num_ccs, nact, nsticky,
-        global, depth, max_path, nlive, dense_levels, table_bytes)."""
+        global, depth, max_path, nlive, dense_levels, naas, shortcuts,
+        table_bytes)."""
         opts = self._plan_opts(precompute_depth, tile_states, tile_mode, max_table_entries)
         n = ctypes.c_int()
         check(lib().ngap_tiles_describe(self._h, ctypes.byref(opts), None, 0, ctypes.byref(n)))
@@ -266,14 +267,15 @@ class Engine:
     def unit_trace(self):
         """Records of the last match's units: numpy structured array with
         fields stream, tile, lo, hi (positions relative to the segment or
-        stream) and work (entries expanded + injected)."""
+        stream), work (entries expanded + injected) and cycles (SM clock
+        cycles the unit's warp spent on it)."""
         n = ctypes.c_int64()
         check(lib().ngap_trace_copy(self._h, None, 0, ctypes.byref(n)))
         cap = max(1, n.value)
         buf = (_lib.UnitTrace * cap)()
         check(lib().ngap_trace_copy(self._h, buf, cap, ctypes.byref(n)))
         dt = np.dtype([("stream", np.int32), ("tile", np.int32), ("lo", np.int64),
-                       ("hi", np.int64), ("work", np.uint64)])
+                       ("hi", np.int64), ("work", np.uint64), ("cycles", np.uint64)])
         return np.frombuffer(buf, dtype=dt, count=n.value).copy()
 
     @property

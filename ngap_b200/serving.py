@@ -354,9 +354,11 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending, light, heavy, nxt = [], [], [], 0
         self._t0 = time.perf_counter()
+        slow = []  # passes of the loop longer than 10 ms: (ms, finish, predict, launch ms)
         while (nxt < len(reqs) or pending or light or heavy
                or any(b is not None for b in self.busy)):
             now = time.perf_counter() - self._t0
+            t_fin = t_pred = t_launch = 0.0
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
                 r = reqs[nxt]
                 nxt += 1
@@ -369,13 +371,17 @@ class Server:
                     self.rejected.append(r)
             for s, b in enumerate(self.busy):
                 if b is not None and self.slots[s].done():
+                    t1 = time.perf_counter()
                     self._finish(s)
+                    t_fin += time.perf_counter() - t1
             # predict as soon as requests arrive (while slots may still be busy,
             # so that the model's cost overlaps the device work), all of them
             # in one call
             if pending:
                 if self.pred is not None:  # one prediction for everything that arrived
+                    t1 = time.perf_counter()
                     rho = self.pred.density(pending)
+                    t_pred += time.perf_counter() - t1
                     chunks = cm.chunk_for(rho, self.rho_ref, self.base_chunk, self.chunk_lo,
                                           self.chunk_hi)
                     for r, d, c in zip(pending, rho, chunks):
@@ -398,16 +404,23 @@ class Server:
                 else:
                     q = heavy if heavy else light
                 if q:
+                    t1 = time.perf_counter()
                     batch = self._form(q, s)
                     if batch:
                         self.slots[s].launch(batch, self._params())
                         self.mem[s] = self.slots[s].memory()
                         self.busy[s] = (batch, now)
+                    t_launch += time.perf_counter() - t1
+            dt = time.perf_counter() - self._t0 - now
+            if dt > 0.01:
+                slow.append((dt * 1e3, t_fin * 1e3, t_pred * 1e3, t_launch * 1e3))
             if (not pending and not light and not heavy and nxt < len(reqs)
                     and all(b is None for b in self.busy)):
                 time.sleep(max(0.0, min(reqs[nxt].arrival - now, 0.0005)))
-        return summarize([r for r in reqs if r.error is None], self.batches,
-                         rejected=len(self.rejected))
+        m = summarize([r for r in reqs if r.error is None], self.batches,
+                      rejected=len(self.rejected))
+        m["slow_passes"] = {"count": len(slow), "longest_ms": sorted(slow, reverse=True)[:5]}
+        return m
 
 
 def summarize(reqs, batches, rejected=0):

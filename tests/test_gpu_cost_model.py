@@ -35,6 +35,8 @@ def test_unit_trace_sums_to_engine_work(engine, small_suite):
     exp, inj = engine.work()
     assert len(tr) > 0 and int(tr["work"].sum()) == exp + inj
     assert np.all(tr["lo"] >= 0) and np.all(tr["hi"] <= lengths[tr["stream"]])
+    # every unit ran: a start clock was replaced by a positive duration (< 2^40)
+    assert np.all(tr["cycles"] > 0) and np.all(tr["cycles"] < (1 << 40))
     # plain matching: positions relative to each segment
     engine.set_trace(True)
     try:

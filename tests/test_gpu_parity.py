@@ -337,6 +337,62 @@ def test_layered_mixed_with_cyclic(engine):
             assert np.array_equal(got, want), (algo, tile_mode)
 
 
+def test_layered_shortcuts(engine):
+    """Successors a `.*` enables from its first match on (their edges from the
+    `.*`'s predecessors dropped from the layered tile): a reporting successor
+    right after the predecessors (gap 0), two predecessors that both lead to
+    the successor (a shortcut) or only one of them (none), over several
+    segments and chunks."""
+    w = W.AnmlWriter()
+    # x y .* z (report at z): y leads to .* and to z
+    w.ste("a0", [ord("x")], ["a1"], start="all-input")
+    w.ste("a1", [ord("y")], ["as", "az"])
+    w.ste("as", None, ["as", "az"], symbol_set="*")
+    w.ste("az", [ord("z")], [], report=True)
+    # (p | q) .* r r, both p and q lead to the first r: a shortcut
+    w.ste("b0", [ord("p")], ["bs", "br"], start="all-input")
+    w.ste("b1", [ord("q")], ["bs", "br"], start="all-input")
+    w.ste("bs", None, ["bs", "br"], symbol_set="*")
+    w.ste("br", [ord("r")], ["bt"])
+    w.ste("bt", [ord("r")], [], report=True)
+    # (p | q) .* z, only p leads to z directly: no shortcut
+    w.ste("c0", [ord("p")], ["cs", "cz"], start="all-input")
+    w.ste("c1", [ord("q")], ["cs"], start="all-input")
+    w.ste("cs", None, ["cs", "cz"], symbol_set="*")
+    w.ste("cz", [ord("z")], [], report=True)
+    groups = nb.Groups(nb.Nfa.from_string(w.text()), group_num=1)
+    lay = [t for t in groups.tiles(precompute_depth=2) if t["phase"] == 2]
+    assert sum(t["shortcuts"] for t in lay) == 2  # az of as, br of bs
+    rng = np.random.default_rng(8)
+    data = rng.choice(np.frombuffer(b"xyzpqr", dtype=np.uint8), size=6000,
+                      p=[0.3, 0.3, 0.1, 0.05, 0.05, 0.2])
+    for algo in ("nonblockingpcgroups", "blockinggroups", "NAPgroups"):
+        for chunk in (0, 97):
+            got, want = run_both(engine, w.text(), data, 6, 1000, depth=2, algorithm=algo,
+                                 chunk=chunk)
+            assert len(want) > 50
+            assert np.array_equal(got, want), (algo, chunk)
+
+
+def test_layered_shortcuts_random(engine):
+    """Random star-heavy automata (extra forward edges around `.*` states,
+    reporting and always-active stars): every layered tile, with or without
+    shortcuts, gives the oracle's reports."""
+    from test_tiles_host import _random_star_nfa
+    with_shortcuts = 0
+    for seed in range(40):
+        rng = np.random.default_rng(500 + seed)
+        anml = _random_star_nfa(rng, int(rng.integers(2, 12)))
+        groups = nb.Groups(nb.Nfa.from_string(anml), group_num=2)
+        with_shortcuts += sum(t["shortcuts"] > 0 for t in groups.tiles(precompute_depth=3))
+        data = rng.integers(96, 102, size=4000).astype(np.uint8)
+        got, want = run_both(engine, anml, data, 4, 1000, group_num=2, depth=3,
+                             algorithm=("nonblockingpcgroups", "blockinggroups")[seed % 2],
+                             chunk=(0, 150)[(seed // 2) % 2])
+        assert np.array_equal(got, want), seed
+    assert with_shortcuts > 5
+
+
 def test_plan_cache_after_tables_freed(engine):
     """Tables created where freed ones were (same address) get their own unit
     plan: the engine keys its plan cache by a serial number."""

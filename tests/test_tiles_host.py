@@ -18,11 +18,77 @@ def _total_ccs_and_states(groups):
     return sum(len(v.cc_begin) - 1 for v in vs), sum(len(v.node_attrs) for v in vs)
 
 
+def _shortcuts(v, nodes, sticky):
+    """Layered tile of a layered CC, restated: for a sticky state s that is
+    not a start-of-data state, with predecessors P (other than s), the
+    successors D of s (not s, not always-active, not sticky) that every state
+    of P leads to; the edges P -> D are dropped (s enables D from its first
+    match on) and the tile keeps the sticky states and the states that reach
+    a report state through the remaining edges (none into always-active or
+    sticky states). Returns (kept states, dropped edges, D per sticky state)."""
+    ro, co = np.asarray(v.row_offsets), np.asarray(v.col_indices)
+    at = np.asarray(v.node_attrs)
+    starts = {int(x) for x in np.asarray(v.start_states)}
+
+    def succ(u):
+        return [int(x) for x in co[ro[u]:ro[u + 1]]]
+    pred = {s: [u for u in nodes if u != s and s in succ(u)] for s in sticky}
+    dropped, dsets = set(), {}
+    for s in sticky:
+        d = set()
+        if pred[s] and s not in starts:
+            d = {u for u in succ(s) if u != s and not at[u] & 1 and u not in sticky
+                 and all(u in succ(x) for x in pred[s])}
+        dsets[s] = d
+        dropped |= {(x, u) for x in pred[s] for u in succ(x) if u in d}
+
+    def kept_edge(x, u):
+        return not at[u] & 1 and u not in sticky and (x, u) not in dropped
+    keep = {u for u in nodes if at[u] & 2}
+    grew = True
+    while grew:
+        grew = False
+        for x in nodes:
+            if x not in keep and any(kept_edge(x, u) and u in keep for u in succ(x)):
+                keep.add(x)
+                grew = True
+    return keep | set(sticky), dropped, dsets
+
+
+def _sticky_of(v, nodes):
+    ro, co = np.asarray(v.row_offsets), np.asarray(v.col_indices)
+    at = np.asarray(v.node_attrs)
+    bits = np.asarray(v.symbol_sets).reshape(-1, 8)
+    return {u for u in nodes if not at[u] & 1 and np.all(bits[u] == 0xFFFFFFFF)
+            and u in co[ro[u]:ro[u + 1]]}
+
+
 def _check_cover(groups, tiles):
-    ccs, states = _total_ccs_and_states(groups)
+    """Every CC lands in one plain tile or one layered pair; plain tiles hold
+    all of a CC's states, layered tiles the states _shortcuts keeps."""
+    ccs, _ = _total_ccs_and_states(groups)
     main = [t for t in tiles if t["phase"] != 1]  # activation tiles repeat part of a pair
     assert sum(t["num_ccs"] for t in main) == ccs
-    assert sum(t["num_states"] for t in main) == states
+    vs = groups.views()
+    kinds = iter(_classify(vs))
+    plain = layered = shortcuts = aas = 0
+    for v in vs:
+        cb = np.asarray(v.cc_begin)
+        at = np.asarray(v.node_attrs)
+        for c in range(len(cb) - 1):
+            nodes = range(int(cb[c]), int(cb[c + 1]))
+            if next(kinds)[0] == "layered":
+                kept, _, dsets = _shortcuts(v, nodes, _sticky_of(v, nodes))
+                layered += len(kept)
+                shortcuts += sum(len(d & kept) for d in dsets.values())
+                aas += sum(1 for u in kept if at[u] & 1)
+            else:
+                plain += len(nodes)
+    lay = [t for t in main if t["phase"] == 2]
+    assert sum(t["num_states"] for t in main if t["phase"] == 0) == plain
+    assert sum(t["num_states"] for t in lay) == layered
+    assert sum(t["shortcuts"] for t in lay) == shortcuts
+    assert sum(t["naas"] for t in lay) == aas
 
 
 @pytest.mark.parametrize("mode", ["auto", "shared", "global"])
@@ -38,7 +104,9 @@ def test_dotstar_pairs(mode):
         a, l = act[k], lay[k]
         assert a["nact"] == l["nact"] == l["nsticky"] == a["num_ccs"] == l["num_ccs"]
         assert a["nsticky"] == 0 and a["max_path"] > 0 and l["max_path"] > 0
-        assert a["num_states"] < l["num_states"]
+        # lit1 . * lit2: lit1's last state leads to the star and to lit2's first
+        # state, a shortcut of the star; lit1's states then leave the layered tile
+        assert l["shortcuts"] == l["nact"] and l["naas"] == 0 and a["naas"] > 0
     # one star per layered CC; the always-active stars make their CCs plain acyclic ones
     non_aas_stars = anml.count('symbol-set="*">')
     assert sum(t["nact"] for t in act.values()) == non_aas_stars
@@ -327,8 +395,9 @@ def _layered_lists(views, keys):
     tables, sticky states they reach, states of the layered tables, their
     report states). Activation tables start from the always-active states
     among the states with a path to a sticky state (through non-sticky
-    states) and stop at sticky states; layered tables start from all
-    always-active states and never enter a sticky state."""
+    states) and stop at sticky states; layered tables start from the
+    always-active states the layered tile keeps (_shortcuts), never enter a
+    sticky state and never take a dropped edge."""
     out = [[set(), 0, set(), set()] for _ in keys]
     for gi, v in enumerate(views):
         ro, co = np.asarray(v.row_offsets), np.asarray(v.col_indices)
@@ -349,6 +418,7 @@ def _layered_lists(views, keys):
             nodes = range(int(cb[c]), int(cb[c + 1]))
             sticky = {u for u in nodes if not at[u] & 1 and np.all(bits[u] == 0xFFFFFFFF)
                       and u in co[ro[u]:ro[u + 1]]}
+            kept, dropped, _ = _shortcuts(v, nodes, sticky)
             pre, grew = set(sticky), True
             while grew:
                 grew = False
@@ -363,9 +433,10 @@ def _layered_lists(views, keys):
                            if x in pre and acc(x, int(b))}
                 out[k][0] |= {u | gi << 22 for u in cur if u not in sticky}
                 out[k][1] += len(cur & sticky)
-                cur = {u for u in nodes if at[u] & 1 and acc(u, int(key[0]))}
+                cur = {u for u in nodes if at[u] & 1 and u in kept and acc(u, int(key[0]))}
                 for b in key[1:]:
-                    cur = {x for u in cur for x in succ(u) if x not in sticky and acc(x, int(b))}
+                    cur = {x for u in cur for x in succ(u) if x not in sticky and x in kept
+                           and (u, x) not in dropped and acc(x, int(b))}
                 out[k][2] |= {u | gi << 22 for u in cur}
                 out[k][3] |= {u | gi << 22 for u in cur if at[u] & 2}
     return out
