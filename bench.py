@@ -768,7 +768,7 @@ SERVE_CHUNKS = dict(adapt_chunks=True, rho_ref=1.0, base_chunk=512, chunk_lo=64,
 
 SERVE_DESC = ("Poisson requests at 2000/s, NFA uniform over the 16 of the batched suite, "
               "length log-normal (median 64 KiB, sigma 1.5, at most 4 MiB), 2 engine slots, "
-              "8 GiB device-memory budget")
+              "16 GiB device-memory budget")
 
 
 def serving_part(args, warmup, suite, steps, step_s=0.25):
@@ -806,7 +806,7 @@ def serving_part(args, warmup, suite, steps, step_s=0.25):
         q = 0
         if pred is not None:
             q = cm.queue_for(float(np.max(pred.density(warm))))
-        srv = sv.Server(s.ts, predictor=pred, slots=2, budget=8 << 30, queue_capacity=q,
+        srv = sv.Server(s.ts, predictor=pred, slots=2, budget=16 << 30, queue_capacity=q,
                         **(SERVE_CHUNKS if pred is not None else {}))
         srv.run([sv.Request(r.rid, r.nfa, r.data, r.arrival) for r in warm])
         servers[name] = (srv, q)

@@ -297,8 +297,10 @@ typedef struct ngap_batch_params {
   int chunk;                /* 0 = automatic */
   int use_graph;            /* capture the pipeline in a CUDA graph; replay it while the
                                tableset, streams, parameters and input pointer repeat */
-  int queue_capacity;       /* overflow-stack entries per warp (>= 1024); 0 = 65536. A run
-                               that needs more fails with NGAP_E_OVERFLOW_QUEUE */
+  int queue_capacity;       /* overflow-stack entries per warp (>= 1024); 0 = 65536. An
+                               engine keeps the largest capacity it has held (a smaller
+                               request runs with that one). A run that needs more fails
+                               with NGAP_E_OVERFLOW_QUEUE */
 } ngap_batch_params;
 
 /* Matches every stream against its NFA in one persistent launch, then sorts

@@ -387,7 +387,11 @@ int ensure_reports(ngap_engine* e, uint64_t cap) {
 int ensure_slots(ngap_engine* e, size_t slots, int max_states, int max_nact, int ovf_cap) {
   int carry_cap = std::max(max_states, 32);
   int mark_words = (max_states + 31) / 32 + 1;
-  if (ovf_cap != e->ovf_cap && e->d_ovf) {  // queue capacity changed: reallocate everything
+  // the overflow stacks only grow: a request for fewer entries than held
+  // keeps them (more room changes no result, while reallocating would
+  // cudaFree, which waits for every stream of the device)
+  if (e->d_ovf && ovf_cap < e->ovf_cap) ovf_cap = e->ovf_cap;
+  if (ovf_cap != e->ovf_cap && e->d_ovf) {  // queue capacity grew: reallocate everything
     e->slots = std::max(e->slots, slots);
     slots = e->slots;
     e->carry_cap = 0;

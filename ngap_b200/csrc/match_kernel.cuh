@@ -927,9 +927,15 @@ __device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem&
 
 // Layered tiles: the work of the unit's sticky states at window offsets
 // [r0, r0 + 32) (lanes over positions). The list holds activation slots
-// (stk_s) and first matches (stk_q); a slot's union mask (the classes any of
-// its successors accepts) rejects most positions before the successor
-// tables are read.
+// (stk_s) and first matches (stk_q). Per group of 32 sticky states, lane k
+// first reads state k's slot, first match and successor record, which the
+// loops below take by shuffle. A first loop tests every state's union mask
+// (the classes any of its successors accepts) at every lane's class: one
+// load per state, independent of each other; a second loop visits only the
+// states some lane passed, each with one load per successor (its class mask
+// word) and a warp prefix sum for the pushes. A state enables its
+// successors after its first match, its shortcut successors (act_local bits
+// 28..31) at it too.
 __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, WarpSmem& ws,
                                                          WarpRun& w, const TileView& tv,
                                                          const UnitCtx& c, int lane, int r0) {
@@ -947,72 +953,59 @@ __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, W
       emit_report(p, ws, w, lane, rs, rs ? __ldg(t.sid + s) : 0u, (uint32_t)tp);
     }
   }
-  // successors of slot i enabled at tp: all of them after its first match,
-  // the shortcut ones (act_local bits 28..31) at it
-  auto enabled = [&](int i, uint32_t al) -> uint32_t {
-    const int64_t q = (int64_t)ws.stk_q[i];
-    return !valid || tp < q ? 0u : (tp > q ? 0xfu : al >> 28);
-  };
   const uint32_t word = sym >> 5, bit = 1u << (sym & 31);
-  int cnt = 0;
-  bool any_rep = false;
-  for (int i = 0; i < w.nstk; i++) {
-    if (!(valid && tp >= (int64_t)ws.stk_q[i])) continue;
-    const uint32_t slot = ws.stk_s[i];
-    if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
-    const uint32_t al = __ldg(t.act_local + slot);
-    const uint32_t on = enabled(i, al);
-    const uint4 sc = load_succ(tv, al & kActIdMask);
-    const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      if (((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym)) {
-        cnt++;
-        any_rep |= (us[j] >> 31) && emit;
-      }
-  }
-  if (__any_sync(kFull, any_rep)) {
-    for (int i = 0; i < w.nstk; i++) {
-      const uint32_t al = __ldg(t.act_local + ws.stk_s[i]);
-      const uint32_t on = enabled(i, al);
-      const uint4 sc = load_succ(tv, al & kActIdMask);
-      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
-      bool ok[4];
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        ok[j] = ((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
-      report4(p, ws, w, tv, lane, ok, us, tp, emit);
+  for (int i0 = 0; i0 < w.nstk; i0 += 32) {
+    const int n = min(32, w.nstk - i0);
+    uint32_t kslot = 0u, kq = 0u, kal = 0u;
+    uint4 ks = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+    if (lane < n) {
+      kslot = ws.stk_s[i0 + lane];
+      kq = ws.stk_q[i0 + lane];
+      kal = __ldg(t.act_local + kslot);
+      ks = load_succ(tv, kal & kActIdMask);
     }
-  }
-  const int pc = need ? cnt : 0;
-  int incl = pc;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int total = __shfl_sync(kFull, incl, 31);
-  if (total == 0) return;
-  if (pc) {
-    int pos = w.top + incl - pc;
-    for (int i = 0; i < w.nstk; i++) {
-      if (tp < (int64_t)ws.stk_q[i]) continue;
-      const uint32_t slot = ws.stk_s[i];
-      if (!(__ldg(t.stk_union + (size_t)slot * tv.cw + word) & bit)) continue;
-      const uint32_t al = __ldg(t.act_local + slot);
-      const uint32_t on = enabled(i, al);
-      const uint4 sc = load_succ(tv, al & kActIdMask);
-      const uint32_t us[4] = {sc.x, sc.y, sc.z, sc.w};
+    // bit k: state i0 + k has matched by this lane's position and some
+    // successor of it accepts the lane's class
+    uint32_t hit = 0u;
+#pragma unroll 4
+    for (int k = 0; k < n; k++) {
+      const uint32_t sl = __shfl_sync(kFull, kslot, k);
+      const uint32_t qk = __shfl_sync(kFull, kq, k);
+      const bool h = valid && tp >= (int64_t)qk &&
+                     (__ldg(t.stk_union + (size_t)sl * tv.cw + word) & bit);
+      hit |= h ? 1u << k : 0u;
+    }
+    uint32_t todo = __reduce_or_sync(kFull, hit);
+    while (todo) {
+      const int k = __ffs(todo) - 1;
+      todo &= todo - 1u;
+      const uint32_t qk = __shfl_sync(kFull, kq, k);
+      const uint32_t al = __shfl_sync(kFull, kal, k);
+      const uint32_t us[4] = {__shfl_sync(kFull, ks.x, k), __shfl_sync(kFull, ks.y, k),
+                              __shfl_sync(kFull, ks.z, k), __shfl_sync(kFull, ks.w, k)};
+      const uint32_t on = !((hit >> k) & 1u) ? 0u : (tp > (int64_t)qk ? 0xfu : al >> 28);
+      bool ok[4];
+      int cnt = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        const uint32_t u = us[j] & kIdMask;
-        if (((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, u, sym))
-          store_entry(p, ws, w, pos++, (u << kEntryPosBits) | (uint32_t)r);
+        ok[j] = ((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
+        cnt += ok[j] && need;
       }
+      report4(p, ws, w, tv, lane, ok, us, tp, emit);
+      int total;
+      const int ex = warp_excl<3>(cnt, lane, total);
+      if (total == 0) continue;
+      if (cnt) {
+        int pos = w.top + ex;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (ok[j] && need)
+            store_entry(p, ws, w, pos++, ((us[j] & kIdMask) << kEntryPosBits) | (uint32_t)r);
+      }
+      grow_stack(p, w, total);
+      __syncwarp();
     }
   }
-  grow_stack(p, w, total);
-  __syncwarp();
 }
 
 // Expands the up-to-32 entries on top of the stack: one step of the worklist.
@@ -1450,8 +1443,17 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       }
       phase[cur] ^= 1u;
       pending[cur] = false;
-      // bytes -> class ids, in place (every tile keys its tables by its own classes)
-      for (uint32_t i = lane; i < nbytes[cur]; i += 32) ws.in[cur][i] = tv.cls[ws.in[cur][i]];
+      // bytes -> class ids, in place (every tile keys its tables by its own
+      // classes); a window whose bytes (look-behind and look-ahead included)
+      // are all of the dead class, which no state of the tile accepts, has
+      // nothing to inject and no sticky work
+      bool live = false;
+      for (uint32_t i = lane; i < nbytes[cur]; i += 32) {
+        const uint8_t k = tv.cls[ws.in[cur][i]];
+        ws.in[cur][i] = k;
+        live |= k < tv.nlive;
+      }
+      live = __any_sync(kFull, live);
       __syncwarp();
       if (we < c.hi)
         nbytes[cur ^ 1] = issue(cur ^ 1, we, c.hi, (int)min((int64_t)defer, we - un.lo), skip[cur ^ 1]);
@@ -1491,10 +1493,12 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
       // the previous window (at most `defer` of them)
       // (without always-active states only plain sticky tiles have injection
       // work: their registered sticky states, batch by batch)
-      int cursor = t->naas == 0 && (LEAN || layered || !tv.sticky) ? c.iend : (int)(inj_pos - wb);
+      int cursor = !live || (t->naas == 0 && (LEAN || layered || !tv.sticky))
+                       ? c.iend
+                       : (int)(inj_pos - wb);
       InjAhead ahead;  // table words of the next batch, read ahead (this window only)
       // layered tiles: next window offset of the sticky states' work
-      int scur = layered && w.nstk > 0 ? 0 : c.wlen;
+      int scur = live && layered && w.nstk > 0 ? 0 : c.wlen;
       while (true) {
         // inject only when the overflow stack is empty, so that it holds at
         // most one batch's excess

@@ -247,7 +247,7 @@ class Server:
                  max_batch_bytes=64 << 20, device=0, queue_capacity=0,
                  algorithm="nonblockingpcgroups", base_chunk=2048, chunk_lo=256, chunk_hi=2048,
                  slot_factory=None, tables_bytes=None, isolate=False, heavy_work=None,
-                 adapt_chunks=True):
+                 adapt_chunks=True, max_batch_requests=256):
         self.ts = tableset
         self.pred = predictor
         self.isolate = bool(isolate and predictor is not None and len(range(slots)) > 1)
@@ -258,27 +258,40 @@ class Server:
         self.chunk_lo, self.chunk_hi = chunk_lo, chunk_hi
         self.budget = budget
         self.max_bytes = max_batch_bytes
+        self.max_requests = max(1, int(max_batch_requests))
         self.queue_capacity = queue_capacity
         self.algorithm = algorithm
         self.rep_cap = max(1 << 16, max_batch_bytes // 4)
         if tables_bytes is None:
             tables_bytes = sum(t.device_bytes for t in getattr(tableset, "tables", []))
         self.tables_bytes = int(tables_bytes)
-        self.max_tiles = max([t.stats()["tiles"] for t in getattr(tableset, "tables", [])] or [1])
+        tiles = [t.stats()["tiles"] for t in getattr(tableset, "tables", [])] or [1]
+        self.max_tiles = max(tiles)
         make = slot_factory or (lambda i: EngineSlot(tableset, device, max_batch_bytes))
         self.slots = [make(i) for i in range(slots)]
         self.busy = [None] * slots      # (batch, launch time)
         self.batches = []               # (size, bytes, predicted work, device ms)
         self.launches = 0               # kernels launched by the served batches
         self.rejected = []              # requests that can never be admitted
-        # allocate each engine's buffers now, for the largest batch (an input
-        # copy of max_batch_bytes, report buffers, per-warp overflow stacks):
-        # a buffer that grew while serving would cost a cudaMalloc, which
-        # waits for the whole device
-        warm = Request(-1, 0, np.zeros(max(16, max_batch_bytes), np.uint8), 0.0)
+        # allocate each engine's buffers now, for the largest batches: an input
+        # copy of max_batch_bytes, report buffers, per-warp overflow stacks,
+        # the unit plan of max_batch_bytes of the NFA with the most tiles at
+        # the shortest chunk, and per-stream rows for max_batch_requests
+        # streams. A buffer that grew while serving would be freed and
+        # allocated again, and cudaFree waits for the whole device, that is
+        # for the other slots' batches too.
+        lo = max(1, int(chunk_lo)) if adapt_chunks else 0
+        big = Request(-1, int(np.argmax(tiles)), np.zeros(max(16, max_batch_bytes), np.uint8), 0.0)
+        big.chunk = lo
+        k = self.max_requests
+        each = max(1, max_batch_bytes // k)
+        many = [Request(-2 - i, i % len(tiles), np.zeros(each, np.uint8), 0.0) for i in range(k)]
+        for r in many:
+            r.chunk = lo
         for sl in self.slots:
-            sl.launch([warm], self._params())
-            sl.finish(1)
+            for warm in ([big], many):
+                sl.launch(warm, self._params())
+                sl.finish(len(warm))
         self.mem = [sl.memory() for sl in self.slots]
         if self.tables_bytes + sum(self._held(m) for m in self.mem) > budget:
             raise ValueError(f"a budget of {budget} bytes does not hold the tables "
@@ -317,7 +330,7 @@ class Server:
         batch fits max_batch_bytes and the device-memory budget (removed from
         queue)."""
         n, nbytes = 0, 0
-        while n < len(queue):
+        while n < len(queue) and n < self.max_requests:
             nb = nbytes + len(queue[n].data)
             if nb > self.max_bytes or not self._fits(s, nb, n + 1):
                 break

@@ -194,14 +194,15 @@ def test_scheduler_knobs_keep_reports(engine, small_suite):
     rng = np.random.default_rng(5)
     chunks = rng.choice([0, 256, 700, 4096, 9000], size=len(offsets))
     for q in (0, 4096, 1024):
+        eng = nb.Engine(0)  # an engine keeps the largest queue it has held
         try:
-            nb.batch_match_async(engine, ts, data, offsets, lengths, nfa_of, chunks=chunks,
+            nb.batch_match_async(eng, ts, data, offsets, lengths, nfa_of, chunks=chunks,
                                  queue_capacity=q)
-            engine.sync()
+            eng.sync()
         except nb.NgapError as ex:
             assert ex.status == 6  # NGAP_E_OVERFLOW_QUEUE
             continue
-        got = nb.batch_results(engine)
+        got = nb.batch_results(eng)
         assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1]), q
 
 
