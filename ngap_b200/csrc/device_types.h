@@ -73,7 +73,7 @@ struct TileDev {
   int32_t depth = 0;        // prefix depth built for this tile (>= 1)
   int32_t max_path = -1;    // longest path in states if acyclic, else -1
   int32_t ncls = 0;         // byte classes
-  int32_t cw = 8;           // class words per state: 1, 2 or 8
+  int32_t cw = 8;           // class-mask words per state: ceil(classes / 32), 1..8
   int32_t nlive = 0;        // live classes: key base; class id nlive = dead
   int32_t narrow = 1;       // 16-bit successors
   int32_t fused = 0;        // wide, one class word: records of 2 x uint4 (successors, their masks)

@@ -76,6 +76,7 @@ struct ngap_tables {
   int64_t bytes = 0;
   int32_t max_states = 0;
   int32_t image_region = 0;  // shared-memory bytes reserved for tile images
+  std::vector<int32_t> plan_bytes;  // per tile: image size of the planning rule (TileHost)
   std::vector<int32_t> pair_nact;  // activation slots of each (activation, layered) tile pair
   int32_t max_nact = 0;            // largest pair
   bool lean = true;                // no tile has sticky states or an activation/layered pass
@@ -303,7 +304,9 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       if ((rc = t->upload(ph.rlist, &pd.rlist)) != NGAP_OK) return rc;
     }
     t->dev_desc.push_back(d);
-    if (d.image_bytes <= to.image_budget) t->image_region = std::max(t->image_region, d.image_bytes);
+    t->plan_bytes.push_back((int32_t)th.plan_bytes);
+    if (th.plan_bytes <= to.image_budget)
+      t->image_region = std::max(t->image_region, (int32_t)th.plan_bytes);
   }
   t->image_region = (t->image_region + 127) & ~127;
   const TileDev* dt = nullptr;
@@ -605,7 +608,7 @@ ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
     }
   }
   const int32_t region = t->image_region;
-  auto is_free = [&](int tile) { return (int32_t)t->tiles[tile].image.size() > region; };
+  auto is_free = [&](int tile) { return t->plan_bytes[tile] > region; };
   make_tasks(units, pass1, unbounded, bounded, grid, is_free, tasks, ntasks1, free_range,
              free_tile);
   return rows;
@@ -1394,7 +1397,7 @@ struct ngap_tableset {
   TileDev* d_tiles = nullptr;
   int ntiles = 0, image_region = 0, max_states = 0, max_groups = 1, max_depth = 1, device = 0;
   int max_nact = 0;
-  std::vector<int32_t> image_bytes;  // per tile of the combined array
+  std::vector<int32_t> plan_bytes;  // per tile of the combined array (planning size)
   bool lean = true;                  // every table lean (see ngap_tables)
   ~ngap_tableset() { cudaFree(d_tiles); }
 };
@@ -1418,7 +1421,7 @@ int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset*
     ts->tables.push_back(t);
     ts->tile_base.push_back((int)all.size());
     all.insert(all.end(), t->dev_desc.begin(), t->dev_desc.end());
-    for (const TileDev& d : t->dev_desc) ts->image_bytes.push_back(d.image_bytes);
+    ts->plan_bytes.insert(ts->plan_bytes.end(), t->plan_bytes.begin(), t->plan_bytes.end());
     ts->lean = ts->lean && t->lean;
     ts->image_region = std::max(ts->image_region, t->image_region);
     ts->max_states = std::max(ts->max_states, t->max_states);
@@ -1536,7 +1539,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
         }
     }
     const int32_t region = ts->image_region;
-    auto is_free = [&](int tile) { return ts->image_bytes[tile] > region; };
+    auto is_free = [&](int tile) { return ts->plan_bytes[tile] > region; };
     make_tasks(units, pass1, unbounded, bounded, full_grid, is_free, tasks, &e->ntasks1,
                e->free_range, e->free_tile);
     if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;

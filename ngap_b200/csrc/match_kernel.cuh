@@ -927,15 +927,16 @@ __device__ __forceinline__ void sticky_positions(const MatchParams& p, WarpSmem&
 
 // Layered tiles: the work of the unit's sticky states at window offsets
 // [r0, r0 + 32) (lanes over positions). The list holds activation slots
-// (stk_s) and first matches (stk_q). Per group of 32 sticky states, lane k
-// first reads state k's slot, first match and successor record, which the
-// loops below take by shuffle. A first loop tests every state's union mask
-// (the classes any of its successors accepts) at every lane's class: one
-// load per state, independent of each other; a second loop visits only the
-// states some lane passed, each with one load per successor (its class mask
-// word) and a warp prefix sum for the pushes. A state enables its
+// (stk_s) and first matches (stk_q). Per group of 32 sticky states: lane k
+// reads state k's slot and first match (its act_local word and first match
+// go to the injection scratch); one loop tests every state's union mask
+// (the classes any successor accepts) at every lane's class, with loads that
+// do not depend on each other; then each lane visits only the states that
+// passed at its position (about two), reads their successor records and
+// pushes the matches through a shared-memory counter. A state enables its
 // successors after its first match, its shortcut successors (act_local bits
-// 28..31) at it too.
+// 28..31) at it too. Reports of successors (rare) take a warp-collective
+// pass afterwards.
 __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, WarpSmem& ws,
                                                          WarpRun& w, const TileView& tv,
                                                          const UnitCtx& c, int lane, int r0) {
@@ -956,14 +957,14 @@ __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, W
   const uint32_t word = sym >> 5, bit = 1u << (sym & 31);
   for (int i0 = 0; i0 < w.nstk; i0 += 32) {
     const int n = min(32, w.nstk - i0);
-    uint32_t kslot = 0u, kq = 0u, kal = 0u;
-    uint4 ks = make_uint4(kNoSucc, kNoSucc, kNoSucc, kNoSucc);
+    uint32_t kslot = 0u, kq = 0u;
     if (lane < n) {
       kslot = ws.stk_s[i0 + lane];
       kq = ws.stk_q[i0 + lane];
-      kal = __ldg(t.act_local + kslot);
-      ks = load_succ(tv, kal & kActIdMask);
+      ws.inj[lane] = __ldg(t.act_local + kslot);
+      ws.inj[32 + lane] = kq;
     }
+    if (lane == 0) ws.inj[64] = 0u;  // entries pushed by the group
     // bit k: state i0 + k has matched by this lane's position and some
     // successor of it accepts the lane's class
     uint32_t hit = 0u;
@@ -975,36 +976,48 @@ __device__ __forceinline__ void layered_sticky_positions(const MatchParams& p, W
                      (__ldg(t.stk_union + (size_t)sl * tv.cw + word) & bit);
       hit |= h ? 1u << k : 0u;
     }
-    uint32_t todo = __reduce_or_sync(kFull, hit);
-    while (todo) {
+    __syncwarp();
+    bool rep = false;
+    for (uint32_t todo = hit; todo; todo &= todo - 1u) {
       const int k = __ffs(todo) - 1;
-      todo &= todo - 1u;
-      const uint32_t qk = __shfl_sync(kFull, kq, k);
-      const uint32_t al = __shfl_sync(kFull, kal, k);
-      const uint32_t us[4] = {__shfl_sync(kFull, ks.x, k), __shfl_sync(kFull, ks.y, k),
-                              __shfl_sync(kFull, ks.z, k), __shfl_sync(kFull, ks.w, k)};
-      const uint32_t on = !((hit >> k) & 1u) ? 0u : (tp > (int64_t)qk ? 0xfu : al >> 28);
+      const uint32_t al = ws.inj[k];
+      const uint32_t on = tp > (int64_t)ws.inj[32 + k] ? 0xfu : al >> 28;
+      const uint4 su = load_succ(tv, al & kActIdMask);
+      const uint32_t us[4] = {su.x, su.y, su.z, su.w};
       bool ok[4];
       int cnt = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         ok[j] = ((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
-        cnt += ok[j] && need;
+        cnt += ok[j];
+        rep |= ok[j] && (us[j] >> 31) && emit;
       }
-      report4(p, ws, w, tv, lane, ok, us, tp, emit);
-      int total;
-      const int ex = warp_excl<3>(cnt, lane, total);
-      if (total == 0) continue;
-      if (cnt) {
-        int pos = w.top + ex;
+      if (need && cnt) {
+        int pos = w.top + (int)atomicAdd(&ws.inj[64], (uint32_t)cnt);
 #pragma unroll
         for (int j = 0; j < 4; j++)
-          if (ok[j] && need)
-            store_entry(p, ws, w, pos++, ((us[j] & kIdMask) << kEntryPosBits) | (uint32_t)r);
+          if (ok[j]) store_entry(p, ws, w, pos++, ((us[j] & kIdMask) << kEntryPosBits) | (uint32_t)r);
       }
-      grow_stack(p, w, total);
-      __syncwarp();
     }
+    __syncwarp();
+    const int total = (int)ws.inj[64];
+    if (__any_sync(kFull, rep)) {  // reports of successors: warp-collective, state by state
+      for (uint32_t any = __reduce_or_sync(kFull, hit); any; any &= any - 1u) {
+        const int k = __ffs(any) - 1;
+        const uint32_t al = ws.inj[k];
+        const uint32_t on = !((hit >> k) & 1u) ? 0u
+                            : (tp > (int64_t)ws.inj[32 + k] ? 0xfu : al >> 28);
+        const uint4 su = load_succ(tv, al & kActIdMask);
+        const uint32_t us[4] = {su.x, su.y, su.z, su.w};
+        bool ok[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          ok[j] = ((on >> j) & 1u) && us[j] != kNoSucc && accepts(tv, us[j] & kIdMask, sym);
+        report4(p, ws, w, tv, lane, ok, us, tp, emit);
+      }
+    }
+    grow_stack(p, w, total);
+    __syncwarp();
   }
 }
 
@@ -1535,7 +1548,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) match_kernel(MatchParams p) {
           if (cursor < c.iend || (!LEAN && scur < c.wlen)) continue;
           break;
         }
-        if (PRIV == 0 && (LEAN || !tv.sticky)) {
+        // (layered tiles have no edge into a sticky state: no successor to register)
+        if (PRIV == 0 && (LEAN || !tv.sticky || layered)) {
           if (tv.fused)
             expand_step2<true>(p, ws, w, tv, c, lane, n_expanded);
           else

@@ -262,7 +262,7 @@ struct Partition {
   }
 };
 
-int class_words(int ncls) { return ncls <= 32 ? 1 : (ncls <= 64 ? 2 : 8); }
+int class_words(int ncls) { return (ncls + 31) / 32; }  // mask words per state: 1..8
 
 inline bool accepts_cls(const TileHost& t, uint32_t v, int c) {
   return (t.cmask[(size_t)v * t.cw + (c >> 5)] >> (c & 31)) & 1u;
@@ -507,6 +507,9 @@ void build_image(TileHost& t) {
   memcpy(t.image.data() + t.off_rep, t.rep.data(), t.rep.size() * 4);
   memcpy(t.image.data() + t.off_sticky, t.sticky.data(), t.sticky.size() * 4);
   memcpy(t.image.data() + t.off_cls, t.cls.data(), 256);
+  const int pcw = plan_class_words(t.ncls);
+  t.plan_bytes = (int64_t)r16(n * (t.narrow ? 8 : (pcw == 1 ? 32 : 16))) + (int64_t)r16(n * pcw * 4) +
+                 2 * (int64_t)r16(((n + 31) / 32) * 4) + 256;
 }
 
 int degree_error() {
@@ -566,10 +569,10 @@ bool emit_tile(const GroupSet& gs, const std::vector<CcInfo>& ccs, bool global, 
   t.cw = class_words(part.n);
   t.cls.resize(256);
   {
-    // bytes no state accepts share one (dead) class; number it last. More
-    // than 64 classes take 8 mask words, but the keys still count only the
-    // live classes, so prefix tables reach one more level within 32-bit keys
-    // than keys over raw bytes (95 printable classes: depth 4 instead of 3)
+    // bytes no state accepts share one (dead) class; number it last. The
+    // keys count only the live classes, so prefix tables reach one more
+    // level within 32-bit keys than keys over raw bytes (95 printable
+    // classes: depth 4 instead of 3)
     uint32_t any[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (size_t ci = 0; ci < ccs.size(); ci++) {
       const CcInfo& c = ccs[ci];
@@ -725,7 +728,7 @@ class TilePacker {
     if (!global_)
       for (int32_t v = ci.begin; v < ci.end; v++) trial.refine(&g.bits[(size_t)v * 8]);
     const bool fits = n_ + sz <= max_states_ &&
-                      (global_ || image_bytes(n_ + sz, class_words(trial.n)) <= opts_.image_budget);
+                      (global_ || image_bytes(n_ + sz, plan_class_words(trial.n)) <= opts_.image_budget);
     if (!open_.empty() && !fits) {
       if (!flush()) return false;
       if (!global_)
@@ -795,7 +798,7 @@ std::vector<std::vector<int>> global_sets_of(const GroupSet& gs, const std::vect
       n += ccs[i].end - ccs[i].begin;
       for (int32_t v = ccs[i].begin; v < ccs[i].end; v++) part.refine(&g.bits[(size_t)v * 8]);
     }
-    if (class_words(part.n) == 1 && image_bytes(n, 1) > two_tiles) {
+    if (plan_class_words(part.n) == 1 && image_bytes(n, 1) > two_tiles) {
       sets.push_back(kv.second);
     } else {
       for (int i : kv.second) {
@@ -806,7 +809,7 @@ std::vector<std::vector<int>> global_sets_of(const GroupSet& gs, const std::vect
       rest_n += n;
     }
   }
-  if (!rest.empty() && image_bytes(rest_n, class_words(rest_part.n)) > two_tiles)
+  if (!rest.empty() && image_bytes(rest_n, plan_class_words(rest_part.n)) > two_tiles)
     sets.push_back(rest);
   return sets;
 }

@@ -43,6 +43,9 @@ struct TileHost {
   std::vector<uint32_t> succ;        // nstates * 4, bit 31 = report successor
   std::vector<uint32_t> bits;        // nstates * 8 raw symbol classes
   std::vector<uint32_t> cmask;       // nstates * cw
+  int64_t plan_bytes = 0;            // the image's size for planning decisions (tile packing,
+                                     // staging): with 1, 2 or 8 mask words, as the planner was
+                                     // tuned, though the image holds ceil(classes / 32)
   std::vector<uint32_t> rep;         // ceil(nstates / 32)
   std::vector<uint32_t> sid;         // nstates: report id, group-local sid | group << 22
   std::vector<uint32_t> aas, start;
@@ -71,6 +74,9 @@ struct TableOpts {
 constexpr int32_t kNarrowMaxStates = 32767;  // 15-bit tile-local ids
 
 // Bytes of a tile image with n states and cw class words.
+// Mask words per state in the planner's size rule (1, 2 or 8).
+inline int plan_class_words(int ncls) { return ncls <= 32 ? 1 : (ncls <= 64 ? 2 : 8); }
+
 inline int64_t image_bytes(int64_t n, int cw) {
   auto r16 = [](int64_t x) { return (x + 15) & ~(int64_t)15; };
   const int64_t succ = n <= kNarrowMaxStates ? n * 8 : n * 16;
