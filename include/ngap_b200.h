@@ -360,6 +360,12 @@ int ngap_mlp_gradient(ngap_mlp* m, const float* x, const float* y, int64_t n, fl
  * activations to bfloat16 (FP32 accumulation); 0 computes in FP32. Runs on
  * the model's own stream; allocates only when n exceeds every earlier call. */
 int ngap_mlp_predict(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y);
+/* The same predictions computed on the host from a host copy of the
+ * parameters (fetched once after each change): for a serving loop, whose GPU
+ * is busy with matching kernels that leave no room for the inference kernel
+ * until they end. Same rounding and accumulation order per unit as the
+ * kernel; the output sum's order differs (FP32 rounding only). */
+int ngap_mlp_predict_host(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y);
 /* Parameters as one FP32 vector; *n = count (out = NULL queries it). */
 int ngap_mlp_get_params(const ngap_mlp* m, float* out, int64_t cap, int64_t* n);
 int ngap_mlp_set_params(ngap_mlp* m, const float* in, int64_t n);

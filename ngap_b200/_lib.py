@@ -171,6 +171,8 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_float)]),
     "ngap_mlp_predict": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                         ctypes.c_int, ctypes.c_void_p]),
+    "ngap_mlp_predict_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                             ctypes.c_int, ctypes.c_void_p]),
     "ngap_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                            ctypes.POINTER(ctypes.c_int64)]),
     "ngap_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),

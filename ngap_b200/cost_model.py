@@ -175,16 +175,18 @@ class LearnedModel:
         self.loss = loss.value
         return self
 
-    def predict_log(self, x, bf16=True):
+    def predict_log(self, x, bf16=True, host=False):
+        """log2(1 + density) per row: the inference kernel, or with host=True
+        the library's host restatement of it (ngap_mlp_predict_host)."""
         xn = self._norm(np.asarray(x, np.float32))
         out = np.zeros(len(xn), np.float32)
         if len(xn):
-            check(lib().ngap_mlp_predict(self._h, xn.ctypes.data, len(xn), int(bool(bf16)),
-                                         out.ctypes.data))
+            fn = lib().ngap_mlp_predict_host if host else lib().ngap_mlp_predict
+            check(fn(self._h, xn.ctypes.data, len(xn), int(bool(bf16)), out.ctypes.data))
         return out
 
-    def predict(self, nfa_of_region, feats, bf16=True):
-        return np.maximum(np.exp2(self.predict_log(feats, bf16)) - 1.0, 0.0)
+    def predict(self, nfa_of_region, feats, bf16=True, host=False):
+        return np.maximum(np.exp2(self.predict_log(feats, bf16, host)) - 1.0, 0.0)
 
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -108,6 +109,19 @@ __global__ void __launch_bounds__(kFeatThreads) features_kernel(const uint8_t* _
 }
 
 // Parameter layout (FP32, contiguous): W1[D][H], b1[H], W2[H][H], b2[H], w3[H], b3.
+// Host rounding of an FP32 value to bfloat16 precision, round to nearest
+// even (the upper 16 bits of the IEEE-754 single after adding half an ulp of
+// bfloat16 plus the tie bit); NaN passes unchanged.
+inline float bf16_round(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) return v;
+  u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
 struct Layout {
   int D, H;
   size_t w1, b1, w2, b2, w3, b3, total;
@@ -311,6 +325,9 @@ struct ngap_mlp {
   float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr, *loss = nullptr;
   __nv_bfloat16* Pb = nullptr;
   bool pb_stale = true;          // Pb needs converting from P
+  // host copy of P for ngap_mlp_predict_host, and its bfloat16-rounded copy
+  std::vector<float> hP, hPb;
+  bool host_stale = true;
   int64_t steps = 0;
   // inference buffers (grow only) and the model's own stream, so that
   // predictions neither allocate nor order against other streams once warm
@@ -473,7 +490,7 @@ int ngap_mlp_train(ngap_mlp* m, const float* x, const float* y, int64_t n, int e
     ngap::set_error("ngap_mlp_train: %s", cudaGetErrorString(ce));
     return NGAP_E_CUDA;
   }
-  m->pb_stale = true;
+  m->pb_stale = m->host_stale = true;
   if (loss) *loss = last / (float)n;
   return NGAP_OK;
 }
@@ -582,7 +599,44 @@ int ngap_mlp_set_params(ngap_mlp* m, const float* in, int64_t n) {
   }
   CM_TRY(cudaSetDevice(m->device));
   CM_TRY(cudaMemcpy(m->P, in, m->L.total * sizeof(float), cudaMemcpyHostToDevice));
-  m->pb_stale = true;
+  m->pb_stale = m->host_stale = true;
+  return NGAP_OK;
+}
+
+int ngap_mlp_predict_host(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y) {
+  if (!m || (n > 0 && (!x || !y)) || n < 0) {
+    ngap::set_error("ngap_mlp_predict_host: bad argument");
+    return NGAP_E_INVALID;
+  }
+  if (n == 0) return NGAP_OK;
+  if (m->host_stale) {  // the parameters changed (training, set_params): fetch them once
+    CM_TRY(cudaSetDevice(m->device));
+    m->hP.resize(m->L.total);
+    CM_TRY(cudaMemcpy(m->hP.data(), m->P, m->L.total * sizeof(float), cudaMemcpyDeviceToHost));
+    m->hPb.resize(m->L.total);
+    for (size_t i = 0; i < m->L.total; i++) m->hPb[i] = bf16_round(m->hP[i]);
+    m->host_stale = false;
+  }
+  const Layout& L = m->L;
+  const float* P = bf16 ? m->hPb.data() : m->hP.data();
+  auto rnd = [bf16](float v) { return bf16 ? bf16_round(v) : v; };
+  std::vector<float> xs(L.D);
+  float h1[kHidden], h2[kHidden];
+  for (int64_t s = 0; s < n; s++) {
+    for (int d = 0; d < L.D; d++) xs[d] = rnd(x[(size_t)s * L.D + d]);
+    // the kernel's accumulation order per unit: bias, then inputs ascending
+    for (int j = 0; j < kHidden; j++) h1[j] = P[L.b1 + j];
+    for (int d = 0; d < L.D; d++)
+      for (int j = 0; j < kHidden; j++) h1[j] = std::fma(xs[d], P[L.w1 + (size_t)d * kHidden + j], h1[j]);
+    for (int j = 0; j < kHidden; j++) h1[j] = rnd(std::max(h1[j], 0.f));
+    for (int j = 0; j < kHidden; j++) h2[j] = P[L.b2 + j];
+    for (int i = 0; i < kHidden; i++)
+      for (int j = 0; j < kHidden; j++) h2[j] = std::fma(h1[i], P[L.w2 + (size_t)i * kHidden + j], h2[j]);
+    for (int j = 0; j < kHidden; j++) h2[j] = rnd(std::max(h2[j], 0.f));
+    float acc = 0.f;
+    for (int i = 0; i < kHidden; i++) acc = std::fma(h2[i], P[L.w3 + i], acc);
+    y[s] = acc + P[L.b3];
+  }
   return NGAP_OK;
 }
 

@@ -147,7 +147,8 @@ def _window_base(nwin, wl):
 class Predictor:
     """Predicted worklist entries of a request: density (entries per byte)
     of its first region times its length. kind: "static" (table rule) or
-    "learned" (MLP, BF16 inference on host features)."""
+    "learned" (the MLP on host features, its BF16 inference run on the host
+    by ngap_mlp_predict_host)."""
 
     def __init__(self, kind, tables, model=None):
         self.kind = kind
@@ -162,7 +163,9 @@ class Predictor:
             return self.static.predict(nf)
         feats = features_host([r.data[:cm.REGION] for r in reqs])
         x = np.concatenate([feats, self.nfeat[nf]], axis=1).astype(np.float32)
-        return self.model.predict(nf, x, bf16=True)
+        # on the host: the matching kernels hold every SM's registers while
+        # batches run, so an inference kernel would wait for them to end
+        return self.model.predict(nf, x, bf16=True, host=True)
 
 
 class EngineSlot:
