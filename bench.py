@@ -824,6 +824,7 @@ def serving_part(args, warmup, suite, steps, step_s=0.25):
             lat[name].append({"p50_ms": m["p50_ms"], "p99_ms": m["p99_ms"],
                               "mean_ms": m["mean_ms"], "batches": m["batches"],
                               "rejected": m["rejected"], "slow_passes": m["slow_passes"],
+                              "host_us_per_request": m["host_us_per_request"],
                               "batch_device_ms_p50": float(np.percentile(dev, 50)),
                               "batch_device_ms_p99": float(np.percentile(dev, 99))})
             served.setdefault(name, []).append(m["MBps"])

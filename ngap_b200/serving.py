@@ -371,6 +371,7 @@ class Server:
         pending, light, heavy, nxt = [], [], [], 0
         self._t0 = time.perf_counter()
         slow = []  # passes of the loop longer than 10 ms: (ms, finish, predict, launch ms)
+        spent = [0.0, 0.0, 0.0]  # seconds in finish, predict and launch over the run
         while (nxt < len(reqs) or pending or light or heavy
                or any(b is not None for b in self.busy)):
             now = time.perf_counter() - self._t0
@@ -428,6 +429,9 @@ class Server:
                         self.busy[s] = (batch, now)
                     t_launch += time.perf_counter() - t1
             dt = time.perf_counter() - self._t0 - now
+            spent[0] += t_fin
+            spent[1] += t_pred
+            spent[2] += t_launch
             if dt > 0.01:
                 slow.append((dt * 1e3, t_fin * 1e3, t_pred * 1e3, t_launch * 1e3))
             if (not pending and not light and not heavy and nxt < len(reqs)
@@ -436,6 +440,9 @@ class Server:
         m = summarize([r for r in reqs if r.error is None], self.batches,
                       rejected=len(self.rejected))
         m["slow_passes"] = {"count": len(slow), "longest_ms": sorted(slow, reverse=True)[:5]}
+        nreq = max(1, len(reqs))
+        m["host_us_per_request"] = {k: 1e6 * v / nreq
+                                    for k, v in zip(("finish", "predict", "launch"), spent)}
         return m
 
 
