@@ -363,8 +363,10 @@ int ngap_mlp_predict(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y)
 /* The same predictions computed on the host from a host copy of the
  * parameters (fetched once after each change): for a serving loop, whose GPU
  * is busy with matching kernels that leave no room for the inference kernel
- * until they end. Same rounding and accumulation order per unit as the
- * kernel; the output sum's order differs (FP32 rounding only). */
+ * until they end. Same bfloat16 roundings and accumulation order per unit as
+ * the kernel, but products and sums rounded apart (no fused multiply-add)
+ * and the output sum in another order: FP32 rounding differences, which a
+ * bfloat16 activation near a rounding boundary can carry to 2^-8 of it. */
 int ngap_mlp_predict_host(ngap_mlp* m, const float* x, int64_t n, int bf16, float* y);
 /* Parameters as one FP32 vector; *n = count (out = NULL queries it). */
 int ngap_mlp_get_params(const ngap_mlp* m, float* out, int64_t cap, int64_t* n);

@@ -624,17 +624,25 @@ int ngap_mlp_predict_host(ngap_mlp* m, const float* x, int64_t n, int bf16, floa
   float h1[kHidden], h2[kHidden];
   for (int64_t s = 0; s < n; s++) {
     for (int d = 0; d < L.D; d++) xs[d] = rnd(x[(size_t)s * L.D + d]);
-    // the kernel's accumulation order per unit: bias, then inputs ascending
+    // the kernel's accumulation order per unit (bias, then inputs ascending),
+    // with products rounded apart: a fused multiply-add without hardware
+    // support is a library call per term, tens of microseconds per row
     for (int j = 0; j < kHidden; j++) h1[j] = P[L.b1 + j];
-    for (int d = 0; d < L.D; d++)
-      for (int j = 0; j < kHidden; j++) h1[j] = std::fma(xs[d], P[L.w1 + (size_t)d * kHidden + j], h1[j]);
+    for (int d = 0; d < L.D; d++) {
+      const float xv = xs[d];
+      const float* wr = P + L.w1 + (size_t)d * kHidden;
+      for (int j = 0; j < kHidden; j++) h1[j] += xv * wr[j];
+    }
     for (int j = 0; j < kHidden; j++) h1[j] = rnd(std::max(h1[j], 0.f));
     for (int j = 0; j < kHidden; j++) h2[j] = P[L.b2 + j];
-    for (int i = 0; i < kHidden; i++)
-      for (int j = 0; j < kHidden; j++) h2[j] = std::fma(h1[i], P[L.w2 + (size_t)i * kHidden + j], h2[j]);
+    for (int i = 0; i < kHidden; i++) {
+      const float hv = h1[i];
+      const float* wr = P + L.w2 + (size_t)i * kHidden;
+      for (int j = 0; j < kHidden; j++) h2[j] += hv * wr[j];
+    }
     for (int j = 0; j < kHidden; j++) h2[j] = rnd(std::max(h2[j], 0.f));
     float acc = 0.f;
-    for (int i = 0; i < kHidden; i++) acc = std::fma(h2[i], P[L.w3 + i], acc);
+    for (int i = 0; i < kHidden; i++) acc += h2[i] * P[L.w3 + i];
     y[s] = acc + P[L.b3];
   }
   return NGAP_OK;

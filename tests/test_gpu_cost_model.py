@@ -137,10 +137,11 @@ def test_mlp_bf16_forward_matches_numpy_rounding():
 
 def test_mlp_host_inference_matches_the_kernel():
     """ngap_mlp_predict_host (the serving loop's inference) against the
-    inference kernel, FP32 and BF16: the hidden layers use the kernel's
-    rounding and accumulation order per unit, only the output sum's order
-    differs, so within 1e-5 of the largest output; it follows parameter
-    changes (set_params)."""
+    inference kernel: the same roundings and accumulation order per unit,
+    products not fused, so FP32 within 1e-4 of the largest output and BF16
+    within 4e-3 (an activation within one bfloat16 step of a rounding
+    boundary may round the other way, as in the BF16 numpy check); it
+    follows parameter changes (set_params)."""
     D = cm.IN_DIM
     m, p, rng = _model(D, 9)
     x = rng.standard_normal((77, D)).astype(np.float32)
@@ -149,12 +150,13 @@ def test_mlp_host_inference_matches_the_kernel():
         host = np.zeros(len(x), np.float32)
         assert nb.lib().ngap_mlp_predict_host(m._h, x.ctypes.data, len(x), int(bf16),
                                               host.ctypes.data) == 0
-        assert np.allclose(host, dev, rtol=1e-5, atol=1e-5 * np.abs(dev).max()), bf16
+        tol = 4e-3 if bf16 else 1e-4
+        assert np.allclose(host, dev, rtol=tol, atol=tol * np.abs(dev).max()), bf16
     m.set_params((p * 0.5).astype(np.float32))
     dev = _raw_predict(m, x, False)
     host = np.zeros(len(x), np.float32)
     nb.lib().ngap_mlp_predict_host(m._h, x.ctypes.data, len(x), 0, host.ctypes.data)
-    assert np.allclose(host, dev, rtol=1e-5, atol=1e-5 * np.abs(dev).max())
+    assert np.allclose(host, dev, rtol=1e-4, atol=1e-4 * np.abs(dev).max())
 
 
 def test_mlp_gradient_matches_numpy_backprop():
