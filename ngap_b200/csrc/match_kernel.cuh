@@ -716,7 +716,9 @@ __device__ __forceinline__ void inject_aas2(const MatchParams& p, WarpSmem& ws, 
   // this batch's list copies and the expansions that follow
   ahead.r0 = -1 << 30;
   const int r1 = r0 + batch;
-  if (AHEAD && r1 < c.iend) {
+  // (only for inline tables, where the word read ahead is the whole lookup;
+  // for the others it would cost a second key computation and no load)
+  if (AHEAD && r1 < c.iend && tv.pt[depth - 1].inline1) {
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       int kn;
