@@ -77,9 +77,9 @@ struct ngap_tables {
   int32_t max_states = 0;
   int32_t image_region = 0;  // shared-memory bytes reserved for tile images
   std::vector<int32_t> plan_bytes;  // per tile: image size of the planning rule (TileHost)
+  std::vector<char> tile_lean;      // per tile: plain, no sticky states (the lean kernel runs it)
   std::vector<int32_t> pair_nact;  // activation slots of each (activation, layered) tile pair
   int32_t max_nact = 0;            // largest pair
-  bool lean = true;                // no tile has sticky states or an activation/layered pass
 
   ~ngap_tables() {
     for (void* p : allocs) cudaFree(p);
@@ -126,8 +126,9 @@ struct ngap_engine {
   size_t tasks_cap = 0;
   int32_t ntasks = 0;
   int32_t ntasks1 = 0;       // tasks of activation tiles, launched first
-  int32_t free_range[4] = {0, 0, 0, 0};  // free units: [begin, count) of each launch
-  int32_t free_tile[2] = {-1, -1};       // the one tile of each launch's free units, or -1
+  int32_t ntasks2 = 0;       // tasks of plain tiles without sticky states (the lean launch)
+  int32_t free_range[6] = {0, 0, 0, 0, 0, 0};  // free units: [begin, count) of each launch
+  int32_t free_tile[3] = {-1, -1, -1};  // the one tile of each launch's free units, or -1
   // worklist traces
   bool trace = false;
   unsigned long long* d_unit_work = nullptr;
@@ -253,7 +254,7 @@ int ngap_tables_build(const ngap_groups* g, const ngap_table_opts* opts, ngap_ta
       return NGAP_E_UNSUPPORTED;
     }
     t->max_states = std::max(t->max_states, th.nstates);
-    t->lean = t->lean && th.nsticky == 0 && th.phase == 0;
+    t->tile_lean.push_back(th.nsticky == 0 && th.phase == 0 ? 1 : 0);
     TileDev d;
     d.group = th.group;
     d.nstates = th.nstates;
@@ -516,23 +517,32 @@ struct ActRows {
 // cyclic tiles first, one per warp of a task; chunks after them in tasks sized
 // to give every CTA several tasks. Units of tiles read in place (is_free)
 // are taken one by one by warps (free units), after the tasks of their
-// launch. Layout of `units`: [activation tasks][activation free]
-// [cyclic tasks][chunk tasks][cyclic free][chunk free]; free_range holds
-// (begin, count) of the free units of the first and of the second launch.
+// launch. Three launches: the activation tiles; the plain tiles without
+// sticky states (is_lean: the lean kernel instance, with fewer registers
+// spilled and a smaller code path); the rest. Layout of `units`, per launch
+// in that order: [cyclic tasks][chunk tasks][cyclic free][chunk free];
+// ntasks1 / ntasks2 count the tasks of the first two launches, free_range
+// holds (begin, count) of each launch's free units.
 void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
                 const std::vector<UnitDev>& unbounded, const std::vector<UnitDev>& bounded,
-                int grid, const std::function<bool(int)>& is_free, std::vector<TaskDev>& tasks,
-                int32_t* ntasks1, int32_t free_range[4], int32_t free_tile[2]) {
+                int grid, const std::function<bool(int)>& is_free,
+                const std::function<bool(int)>& is_lean, std::vector<TaskDev>& tasks,
+                int32_t* ntasks1, int32_t* ntasks2, int32_t free_range[6], int32_t free_tile[3]) {
   units.clear();
   tasks.clear();
   auto split = [&](const std::vector<UnitDev>& src, std::vector<UnitDev>& st,
                    std::vector<UnitDev>& fr) {
     for (const UnitDev& u : src) (is_free(u.tile) ? fr : st).push_back(u);
   };
-  std::vector<UnitDev> p1s, p1f, ubs, ubf, bs, bf;
+  std::vector<UnitDev> p1s, p1f, ubs, ubf, bs, bf, lubs, lubf, lbs, lbf;
   split(pass1, p1s, p1f);
-  split(unbounded, ubs, ubf);
-  split(bounded, bs, bf);
+  std::vector<UnitDev> lean_ub, lean_b, rest_ub, rest_b;
+  for (const UnitDev& u : unbounded) (is_lean(u.tile) ? lean_ub : rest_ub).push_back(u);
+  for (const UnitDev& u : bounded) (is_lean(u.tile) ? lean_b : rest_b).push_back(u);
+  split(lean_ub, lubs, lubf);
+  split(lean_b, lbs, lbf);
+  split(rest_ub, ubs, ubf);
+  split(rest_b, bs, bf);
   // a launch whose free units all belong to one tile: its CTAs stage that
   // tile's descriptors in shared memory once
   auto one_tile = [](const std::vector<UnitDev>& a, const std::vector<UnitDev>& b) {
@@ -545,7 +555,8 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
     return tile;
   };
   free_tile[0] = one_tile(p1f, {});
-  free_tile[1] = one_tile(ubf, bf);
+  free_tile[1] = one_tile(lubf, lbf);
+  free_tile[2] = one_tile(ubf, bf);
   auto per = [&](size_t n) {
     return std::max<int64_t>(kWarpsPerCta,
                              std::min<int64_t>(512, (int64_t)n / std::max(1, 4 * grid)));
@@ -585,18 +596,25 @@ void make_tasks(std::vector<UnitDev>& units, const std::vector<UnitDev>& pass1,
   *ntasks1 = (int32_t)tasks.size();
   free_range[0] = (int32_t)append(p1f);
   free_range[1] = (int32_t)p1f.size();
-  b = append(ubs);
-  cut(b, units.size(), kWarpsPerCta);
-  b = append(bs);
-  cut(b, units.size(), per(bs.size()));
-  free_range[2] = (int32_t)append(ubf);
-  append(bf);
-  free_range[3] = (int32_t)(ubf.size() + bf.size());
+  auto launch = [&](const std::vector<UnitDev>& cs, const std::vector<UnitDev>& chs,
+                    const std::vector<UnitDev>& cf, const std::vector<UnitDev>& chf,
+                    int32_t* fr) {
+    size_t bb = append(cs);
+    cut(bb, units.size(), kWarpsPerCta);
+    bb = append(chs);
+    cut(bb, units.size(), per(chs.size()));
+    fr[0] = (int32_t)append(cf);
+    append(chf);
+    fr[1] = (int32_t)(cf.size() + chf.size());
+  };
+  launch(lubs, lbs, lubf, lbf, free_range + 2);
+  *ntasks2 = (int32_t)tasks.size() - *ntasks1;
+  launch(ubs, bs, ubf, bf, free_range + 4);
 }
 
 ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
                    std::vector<UnitDev>& units, std::vector<TaskDev>& tasks, int32_t* ntasks1,
-                   int32_t free_range[4], int32_t free_tile[2]) {
+                   int32_t* ntasks2, int32_t free_range[6], int32_t free_tile[3]) {
   std::vector<UnitDev> pass1, unbounded, bounded;
   ActRows rows({t}, k.num_seg);
   for (int ti = 0; ti < (int)t->tiles.size(); ti++) {
@@ -609,8 +627,9 @@ ActRows plan_units(const ngap_tables* t, const UnitPlanKey& k, int grid,
   }
   const int32_t region = t->image_region;
   auto is_free = [&](int tile) { return t->plan_bytes[tile] > region; };
-  make_tasks(units, pass1, unbounded, bounded, grid, is_free, tasks, ntasks1, free_range,
-             free_tile);
+  auto is_lean = [&](int tile) { return t->tile_lean[tile] != 0; };
+  make_tasks(units, pass1, unbounded, bounded, grid, is_free, is_lean, tasks, ntasks1, ntasks2,
+             free_range, free_tile);
   return rows;
 }
 
@@ -702,58 +721,54 @@ int launch_grid(const ngap_engine* e, int ntasks, int nfree) {
 
 int plan_grid(const ngap_engine* e, int full_grid) {
   const int64_t want = (int64_t)e->ntasks +
-                       ((int64_t)e->free_range[1] + e->free_range[3] + kWarpsPerCta - 1) / kWarpsPerCta;
+                       ((int64_t)e->free_range[1] + e->free_range[3] + e->free_range[5] +
+                        kWarpsPerCta - 1) / kWarpsPerCta;
   return (int)std::max<int64_t>(1, std::min<int64_t>(full_grid, want));
 }
 
-// The matching launches of a plan: the activation tiles' work, then the rest
+// The matching launches of a plan: the activation tiles' work; the plain
+// tiles without sticky states in the lean kernel instance; then the rest
 // (the layered tiles read what the first launch recorded). Each launch takes
 // its tasks first, then its free units.
-template <int PRIV, bool LEAN>
+template <int PRIV>
 int launch_plan(ngap_engine* e, MatchParams mp, int smem, cudaStream_t st) {
-  unsigned int* free_cursor = e->d_unit_counter + 1;
-  mp.free_cursor = free_cursor;
+  mp.free_cursor = e->d_unit_counter + 1;
+  const TaskDev* const tasks0 = mp.tasks;
   if (e->act_entries > 0)
     CUDA_TRY(cudaMemsetAsync(e->d_act, 0xff, (size_t)e->act_entries * sizeof(uint32_t), st));
-  if (e->ntasks1 > 0 || e->free_range[1] > 0) {
-    mp.ntasks = e->ntasks1;
-    mp.free_begin = e->free_range[0];
-    mp.nfree = e->free_range[1];
-    mp.free_tile = e->free_tile[0];
+  auto run = [&](bool lean, int32_t tbegin, int32_t ntasks, int which) -> int {
+    const int32_t nfree = e->free_range[2 * which + 1];
+    if (ntasks == 0 && nfree == 0) return NGAP_OK;
+    mp.tasks = tasks0 + tbegin;
+    mp.ntasks = ntasks;
+    mp.free_begin = e->free_range[2 * which];
+    mp.nfree = nfree;
+    mp.free_tile = e->free_tile[which];
     CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, 2 * sizeof(unsigned int), st));
-    match_kernel<PRIV, LEAN><<<launch_grid(e, mp.ntasks, mp.nfree), kCtaThreads, smem, st>>>(mp);
+    const int grid = launch_grid(e, ntasks, nfree);
+    if (lean)
+      match_kernel<PRIV, true><<<grid, kCtaThreads, smem, st>>>(mp);
+    else
+      match_kernel<PRIV, false><<<grid, kCtaThreads, smem, st>>>(mp);
     CUDA_TRY(cudaGetLastError());
     e->launches++;
-  }
+    return NGAP_OK;
+  };
+  int rc = run(false, 0, e->ntasks1, 0);
+  if (rc == NGAP_OK) rc = run(true, e->ntasks1, e->ntasks2, 1);
+  if (rc != NGAP_OK) return rc;
   if (e->act_rows > 0) {
     act_compact<<<(e->act_rows + 7) / 8, 256, 0, st>>>(e->d_row_off, e->d_row_n, e->act_rows,
                                                        e->d_act, e->d_act_list, e->d_act_cnt);
     CUDA_TRY(cudaGetLastError());
     e->launches++;
   }
-  if (e->ntasks > e->ntasks1 || e->free_range[3] > 0) {
-    mp.tasks = e->d_tasks + e->ntasks1;
-    mp.ntasks = e->ntasks - e->ntasks1;
-    mp.free_begin = e->free_range[2];
-    mp.nfree = e->free_range[3];
-    mp.free_tile = e->free_tile[1];
-    CUDA_TRY(cudaMemsetAsync(e->d_unit_counter, 0, 2 * sizeof(unsigned int), st));
-    match_kernel<PRIV, LEAN><<<launch_grid(e, mp.ntasks, mp.nfree), kCtaThreads, smem, st>>>(mp);
-    CUDA_TRY(cudaGetLastError());
-    e->launches++;
-  }
-  return NGAP_OK;
+  return run(false, e->ntasks1 + e->ntasks2, e->ntasks - e->ntasks1 - e->ntasks2, 2);
 }
 
-int launch_any(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t st, int priv,
-               bool lean) {
-  if (lean)
-    return priv == 0 ? launch_plan<0, true>(e, mp, smem, st)
-                     : priv == 1 ? launch_plan<1, true>(e, mp, smem, st)
-                                 : launch_plan<2, true>(e, mp, smem, st);
-  return priv == 0 ? launch_plan<0, false>(e, mp, smem, st)
-                   : priv == 1 ? launch_plan<1, false>(e, mp, smem, st)
-                               : launch_plan<2, false>(e, mp, smem, st);
+int launch_any(ngap_engine* e, const MatchParams& mp, int smem, cudaStream_t st, int priv) {
+  return priv == 0 ? launch_plan<0>(e, mp, smem, st)
+                   : priv == 1 ? launch_plan<1>(e, mp, smem, st) : launch_plan<2>(e, mp, smem, st);
 }
 
 __global__ void swap_halves(uint64_t* a, uint64_t n) {
@@ -1082,10 +1097,11 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   if (e->plan_tables != t->serial || key < e->plan_key || e->plan_key < key) {
     std::vector<UnitDev> units;
     std::vector<TaskDev> tasks;
-    int32_t ntasks1 = 0;
-    const ActRows rows = plan_units(t, key, full_grid, units, tasks, &ntasks1, e->free_range,
-                                    e->free_tile);
+    int32_t ntasks1 = 0, ntasks2 = 0;
+    const ActRows rows = plan_units(t, key, full_grid, units, tasks, &ntasks1, &ntasks2,
+                                    e->free_range, e->free_tile);
     e->ntasks1 = ntasks1;
+    e->ntasks2 = ntasks2;
     if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       const size_t cap = grown(e->units_cap, units.size());
@@ -1168,8 +1184,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   if ((rc = trace_buffer(e, st, &mp.unit_work, &mp.unit_cycles)) != NGAP_OK) return rc;
   e->trace_seg_len = p->seg_len;
   CUDA_TRY(cudaEventRecord(e->ev[1], st));
-  if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0) {
-    rc = launch_any(e, mp, smem, st, priv, t->lean);
+  if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0 || e->free_range[5] > 0) {
+    rc = launch_any(e, mp, smem, st, priv);
     if (rc != NGAP_OK) return rc;
   }
   CUDA_TRY(cudaEventRecord(e->ev[2], st));
@@ -1398,7 +1414,7 @@ struct ngap_tableset {
   int ntiles = 0, image_region = 0, max_states = 0, max_groups = 1, max_depth = 1, device = 0;
   int max_nact = 0;
   std::vector<int32_t> plan_bytes;  // per tile of the combined array (planning size)
-  bool lean = true;                  // every table lean (see ngap_tables)
+  std::vector<char> tile_lean;      // per tile of the combined array (ngap_tables::tile_lean)
   ~ngap_tableset() { cudaFree(d_tiles); }
 };
 
@@ -1422,7 +1438,7 @@ int ngap_tableset_create(const ngap_tables* const* tables, int n, ngap_tableset*
     ts->tile_base.push_back((int)all.size());
     all.insert(all.end(), t->dev_desc.begin(), t->dev_desc.end());
     ts->plan_bytes.insert(ts->plan_bytes.end(), t->plan_bytes.begin(), t->plan_bytes.end());
-    ts->lean = ts->lean && t->lean;
+    ts->tile_lean.insert(ts->tile_lean.end(), t->tile_lean.begin(), t->tile_lean.end());
     ts->image_region = std::max(ts->image_region, t->image_region);
     ts->max_states = std::max(ts->max_states, t->max_states);
     ts->max_groups = std::max(ts->max_groups, t->num_groups);
@@ -1540,8 +1556,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     }
     const int32_t region = ts->image_region;
     auto is_free = [&](int tile) { return ts->plan_bytes[tile] > region; };
-    make_tasks(units, pass1, unbounded, bounded, full_grid, is_free, tasks, &e->ntasks1,
-               e->free_range, e->free_tile);
+    auto is_lean = [&](int tile) { return ts->tile_lean[tile] != 0; };
+    make_tasks(units, pass1, unbounded, bounded, full_grid, is_free, is_lean, tasks, &e->ntasks1,
+               &e->ntasks2, e->free_range, e->free_tile);
     if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       const size_t cap = grown(e->units_cap, units.size());
@@ -1629,8 +1646,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     CUDA_TRY(cudaMemsetAsync(e->d_counters, 0, 8 * sizeof(unsigned long long), qs));
     CUDA_TRY(cudaMemsetAsync(e->d_err, 0, sizeof(int), qs));
     int r = NGAP_OK;
-    if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0) {
-      r = launch_any(e, mp, smem, qs, priv, ts->lean);
+    if (e->ntasks > 0 || e->free_range[1] > 0 || e->free_range[3] > 0 || e->free_range[5] > 0) {
+      r = launch_any(e, mp, smem, qs, priv);
       if (r != NGAP_OK) return r;
     }
     if (!p->report_off) {
