@@ -182,11 +182,13 @@ class EngineSlot:
         self.pinned = torch.empty(max_batch_bytes, dtype=torch.uint8).pin_memory()
         self.event = None
         self.args = None
+        self.spent = [0.0, 0.0]  # seconds copying requests into the staging buffer, in the match call
 
     def memory(self):
         return self.engine.memory()
 
     def launch(self, batch, params):
+        t0 = time.perf_counter()
         buf = self.pinned.numpy()
         offs = np.zeros(len(batch), np.int64)
         lens = np.array([len(r.data) for r in batch], np.int64)
@@ -198,7 +200,10 @@ class EngineSlot:
         nfa = np.array([r.nfa for r in batch], np.int32)
         kw = dict(params, stream=self.stream.cuda_stream,
                   chunks=np.array([r.chunk for r in batch], np.int64))
+        t1 = time.perf_counter()
         batch_match_async(self.engine, self.ts, buf[:pos], offs, lens, nfa, **kw)
+        self.spent[0] += t1 - t0
+        self.spent[1] += time.perf_counter() - t1
         self.event = self.torch.cuda.Event()
         self.event.record(self.stream)
         self.args = (offs, lens, nfa, kw, pos)
@@ -369,6 +374,8 @@ class Server:
         share a batch with (and wait for) a predicted-heavy one."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending, light, heavy, nxt = [], [], [], 0
+        self._spent0 = [sum(getattr(sl, "spent", [0.0, 0.0])[i] for sl in self.slots)
+                        for i in range(2)]
         self._t0 = time.perf_counter()
         slow = []  # passes of the loop longer than 10 ms: (ms, finish, predict, launch ms)
         spent = [0.0, 0.0, 0.0]  # seconds in finish, predict and launch over the run
@@ -443,6 +450,11 @@ class Server:
         nreq = max(1, len(reqs))
         m["host_us_per_request"] = {k: 1e6 * v / nreq
                                     for k, v in zip(("finish", "predict", "launch"), spent)}
+        # launch, split: copying requests into the slots' staging buffers and
+        # the batched match call itself (plan, copies, kernel launches)
+        split = [sum(getattr(sl, "spent", [0.0, 0.0])[i] for sl in self.slots) for i in range(2)]
+        m["host_us_per_request"].update({"launch_copy": 1e6 * (split[0] - self._spent0[0]) / nreq,
+                                         "launch_match_call": 1e6 * (split[1] - self._spent0[1]) / nreq})
         return m
 
 
