@@ -166,6 +166,12 @@ struct ngap_engine {
   size_t slots = 0;
   int carry_cap = 0, mark_words = 0, ovf_cap = 0;
   int max_smem_set = -1;
+  int bps_smem[3] = {-1, -1, -1}, bps_val[3] = {0, 0, 0};  // resident CTAs per SM, per PRIV
+  // pinned staging of plan uploads (grow-only) and the event of the last one
+  uint8_t* h_plan = nullptr;
+  size_t h_plan_cap = 0;
+  cudaEvent_t plan_ev = nullptr;
+  bool plan_ev_pending = false;
   // timing
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float match_ms = 0.f, sort_ms = 0.f;
@@ -226,6 +232,9 @@ struct ngap_engine {
     if (h_counters) cudaFreeHost(h_counters);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    if (plan_ev) cudaEventSynchronize(plan_ev);
+    if (plan_ev) cudaEventDestroy(plan_ev);
+    if (h_plan) cudaFreeHost(h_plan);
   }
 };
 
@@ -367,6 +376,56 @@ namespace {
 template <class T>
 T grown(T cap, T need) {
   return std::max(need, cap * 2);
+}
+
+// One host array to copy to a device buffer.
+struct Upload {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+// Copies plan arrays to the device on stream st through the engine's pinned
+// staging buffer, so that the host does not wait: a synchronous copy from
+// pageable memory queues behind other streams' transfers on the copy
+// engine (in a serving loop, the other slot's input copy). The staging
+// buffer is written again only once the last upload has ended (an event).
+// Inside a stream capture the copies stay synchronous, so that no captured
+// node reads the reusable staging buffer.
+int upload_plan(ngap_engine* e, cudaStream_t st, const std::vector<Upload>& parts) {
+  size_t total = 0;
+  for (const Upload& u : parts) total += (u.bytes + 15) & ~(size_t)15;
+  if (total == 0) return NGAP_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    for (const Upload& u : parts)
+      if (u.bytes) CUDA_TRY(cudaMemcpy(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice));
+    return NGAP_OK;
+  }
+  if (e->plan_ev_pending) {
+    CUDA_TRY(cudaEventSynchronize(e->plan_ev));
+    e->plan_ev_pending = false;
+  }
+  if (total > e->h_plan_cap) {
+    const size_t cap = grown(e->h_plan_cap, total);
+    if (e->h_plan) cudaFreeHost(e->h_plan);
+    e->h_plan = nullptr;
+    e->h_plan_cap = 0;
+    CUDA_TRY(cudaMallocHost(&e->h_plan, cap));
+    e->h_plan_cap = cap;
+  }
+  if (!e->plan_ev) CUDA_TRY(cudaEventCreateWithFlags(&e->plan_ev, cudaEventDisableTiming));
+  size_t off = 0;
+  for (const Upload& u : parts) {
+    if (u.bytes == 0) continue;
+    std::memcpy(e->h_plan + off, u.src, u.bytes);
+    CUDA_TRY(cudaMemcpyAsync(u.dst, e->h_plan + off, u.bytes, cudaMemcpyHostToDevice, st));
+    off += (u.bytes + 15) & ~(size_t)15;
+  }
+  CUDA_TRY(cudaEventRecord(e->plan_ev, st));
+  e->plan_ev_pending = true;
+  return NGAP_OK;
 }
 
 int ensure_reports(ngap_engine* e, uint64_t cap) {
@@ -654,7 +713,7 @@ int trace_buffer(ngap_engine* e, cudaStream_t st, unsigned long long** work,
 }
 
 // Activation buffers of a plan (slots, compacted lists, row table).
-int set_act_rows(ngap_engine* e, const ActRows& rows) {
+int set_act_rows(ngap_engine* e, const ActRows& rows, std::vector<Upload>& ups) {
   e->act_entries = rows.total;
   e->act_rows = (int32_t)rows.row_off.size();
   if (e->act_entries > e->act_cap) {
@@ -682,10 +741,8 @@ int set_act_rows(ngap_engine* e, const ActRows& rows) {
     e->rows_cap = cap;
   }
   if (e->act_rows > 0) {
-    CUDA_TRY(cudaMemcpy(e->d_row_off, rows.row_off.data(), rows.row_off.size() * sizeof(int64_t),
-                        cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(e->d_row_n, rows.row_n.data(), rows.row_n.size() * sizeof(int32_t),
-                        cudaMemcpyHostToDevice));
+    ups.push_back({e->d_row_off, rows.row_off.data(), rows.row_off.size() * sizeof(int64_t)});
+    ups.push_back({e->d_row_n, rows.row_n.data(), rows.row_n.size() * sizeof(int32_t)});
   }
   return NGAP_OK;
 }
@@ -816,6 +873,22 @@ int blocks_per_sm(int smem, int* out) {
     return NGAP_E_CUDA;
   }
   return NGAP_OK;
+}
+
+// blocks_per_sm of the engine's last shared-memory size per algorithm (the
+// occupancy query costs a driver call on every match otherwise).
+int cached_blocks_per_sm(ngap_engine* e, int priv, int smem, int* out) {
+  if (e->bps_smem[priv] == smem) {
+    *out = e->bps_val[priv];
+    return NGAP_OK;
+  }
+  const int rc = priv == 0 ? blocks_per_sm<0>(smem, out)
+                 : priv == 1 ? blocks_per_sm<1>(smem, out) : blocks_per_sm<2>(smem, out);
+  if (rc == NGAP_OK) {
+    e->bps_smem[priv] = smem;
+    e->bps_val[priv] = *out;
+  }
+  return rc;
 }
 
 // One sort of report keys: d_in[0 .. *d_n) (clamped to cap) into unique
@@ -1088,8 +1161,7 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   const int smem = cta_smem_bytes(window, t->image_region);
   if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
   int bps = 0;
-  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
-                                                              : blocks_per_sm<2>(smem, &bps);
+  rc = cached_blocks_per_sm(e, priv, smem, &bps);
   if (rc != NGAP_OK) return rc;
   const int full_grid = e->num_sms * bps;
   // units and tasks
@@ -1102,7 +1174,8 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
                                     e->free_range, e->free_tile);
     e->ntasks1 = ntasks1;
     e->ntasks2 = ntasks2;
-    if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
+    std::vector<Upload> ups;
+    if ((rc = set_act_rows(e, rows, ups)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       const size_t cap = grown(e->units_cap, units.size());
       cudaFree(e->d_units);
@@ -1119,12 +1192,9 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
       CUDA_TRY(cudaMalloc(&e->d_tasks, cap * sizeof(TaskDev)));
       e->tasks_cap = cap;
     }
-    if (!units.empty())
-      CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
-                          cudaMemcpyHostToDevice));
-    if (!tasks.empty())
-      CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
-                          cudaMemcpyHostToDevice));
+    if (!units.empty()) ups.push_back({e->d_units, units.data(), units.size() * sizeof(UnitDev)});
+    if (!tasks.empty()) ups.push_back({e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev)});
+    if ((rc = upload_plan(e, st, ups)) != NGAP_OK) return rc;
     e->nunits = (int32_t)units.size();
     e->h_units = units;
     e->ntasks = (int32_t)tasks.size();
@@ -1501,8 +1571,7 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   const int smem = cta_smem_bytes(window, ts->image_region);
   if ((rc = set_smem(e, smem)) != NGAP_OK) return rc;
   int bps = 0;
-  rc = priv == 0 ? blocks_per_sm<0>(smem, &bps) : priv == 1 ? blocks_per_sm<1>(smem, &bps)
-                                                              : blocks_per_sm<2>(smem, &bps);
+  rc = cached_blocks_per_sm(e, priv, smem, &bps);
   if (rc != NGAP_OK) return rc;
   const int full_grid = e->num_sms * bps;
   // buffers (before any capture)
@@ -1559,7 +1628,8 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
     auto is_lean = [&](int tile) { return ts->tile_lean[tile] != 0; };
     make_tasks(units, pass1, unbounded, bounded, full_grid, is_free, is_lean, tasks, &e->ntasks1,
                &e->ntasks2, e->free_range, e->free_tile);
-    if ((rc = set_act_rows(e, rows)) != NGAP_OK) return rc;
+    std::vector<Upload> ups;
+    if ((rc = set_act_rows(e, rows, ups)) != NGAP_OK) return rc;
     if (units.size() > e->units_cap) {
       const size_t cap = grown(e->units_cap, units.size());
       cudaFree(e->d_units);
@@ -1576,12 +1646,9 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
       CUDA_TRY(cudaMalloc(&e->d_tasks, cap * sizeof(TaskDev)));
       e->tasks_cap = cap;
     }
-    if (!units.empty())
-      CUDA_TRY(cudaMemcpy(e->d_units, units.data(), units.size() * sizeof(UnitDev),
-                          cudaMemcpyHostToDevice));
-    if (!tasks.empty())
-      CUDA_TRY(cudaMemcpy(e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev),
-                          cudaMemcpyHostToDevice));
+    if (!units.empty()) ups.push_back({e->d_units, units.data(), units.size() * sizeof(UnitDev)});
+    if (!tasks.empty()) ups.push_back({e->d_tasks, tasks.data(), tasks.size() * sizeof(TaskDev)});
+    if ((rc = upload_plan(e, st, ups)) != NGAP_OK) return rc;
     e->nunits = (int32_t)units.size();
     e->h_units = units;
     e->ntasks = (int32_t)tasks.size();
