@@ -148,6 +148,24 @@ def _reqs(sizes):
     return [sv.Request(i, 0, np.zeros(n, np.uint8), 0.0) for i, n in enumerate(sizes)]
 
 
+def test_serving_warmup_and_request_cap():
+    """Each slot is warmed with the largest plan (one max_batch_bytes request
+    of the NFA with the most tiles at the shortest chunk) and with the most
+    streams (max_batch_requests requests), so that no buffer grows while
+    serving; a batch never holds more than max_batch_requests requests."""
+    made = []
+
+    def factory(i):
+        made.append(FakeSlot(1000))
+        return made[-1]
+    srv = sv.Server(None, slots=2, budget=1 << 20, max_batch_bytes=1000, chunk_lo=64,
+                    slot_factory=factory, tables_bytes=100, max_batch_requests=4)
+    for sl in made:
+        assert [len(b) for b in sl.launched] == [1, 4]  # the big request, then the many
+    q = _reqs([10] * 9)
+    assert len(srv._form(q, 0)) == 4 and len(q) == 5
+
+
 def test_serving_admission_counts_engine_buffers():
     # tables 100 + fixed 1000 + the warm-up batch's input copy of max_batch_bytes
     # (1000 B -> 1072): every engine buffer is allocated at construction

@@ -337,6 +337,26 @@ def test_layered_mixed_with_cyclic(engine):
             assert np.array_equal(got, want), (algo, tile_mode)
 
 
+def test_dead_windows(engine):
+    """Windows whose bytes are all of the tile's dead class (bytes no state
+    accepts) skip injection: DNA patterns over a stream of 'x' with ACGT
+    islands (planted occurrences included) that straddle window and chunk
+    boundaries, matches carried into dead windows among them."""
+    anml, dna = W.hamming_set(seed=61, n_patterns=20, input_len=1 << 14, plant_every=1 << 9)
+    rng = np.random.default_rng(61)
+    data = np.full(1 << 16, ord("x"), dtype=np.uint8)
+    for _ in range(200):
+        n = int(rng.integers(20, 600))
+        at = int(rng.integers(0, len(data) - n))
+        src = int(rng.integers(0, len(dna) - n))
+        data[at:at + n] = dna[src:src + n]
+    for window, chunk in ((64, 0), (0, 700), (97, 300)):
+        got, want = run_both(engine, anml, data, 4, len(data) // 4, group_num=2, depth=-1,
+                             algorithm="nonblockingpcgroups", window=window, chunk=chunk)
+        assert len(want) > 20
+        assert np.array_equal(got, want), (window, chunk)
+
+
 def test_layered_shortcuts(engine):
     """Successors a `.*` enables from its first match on (their edges from the
     `.*`'s predecessors dropped from the layered tile): a reporting successor
