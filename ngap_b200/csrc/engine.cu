@@ -1009,7 +1009,7 @@ int sort_reports(ngap_engine* e, const SortJob& j, cudaStream_t st) {
     for (auto& g : e->sort_graphs)
       if (g.key == key) sg = &g;
     if (!sg) {
-      if (e->sort_graphs.size() >= 8) {  // keep a few configurations
+      if (e->sort_graphs.size() >= 16) {  // keep a few configurations
         e->sort_graphs.front().release();
         e->sort_graphs.erase(e->sort_graphs.begin());
       }
@@ -1552,8 +1552,16 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   }
   // report key: stream | offset in stream | id
   const int ibits = 22 + bits_for((uint64_t)std::max(ts->max_groups, 1));
-  const int obits = bits_for(max_len);
-  const int sbits = bits_for((uint64_t)nstreams);
+  int obits = bits_for(max_len);
+  int sbits = bits_for((uint64_t)nstreams);
+  // field widths rounded up to the radix digit (4 bits) when the key still
+  // fits: the same number of radix passes and far fewer distinct layouts, so
+  // that the sort's CUDA graph (keyed by the layout) is reused across batches
+  // of other lengths and stream counts instead of being captured again
+  if (ibits + ((obits + 3) & ~3) + ((sbits + 3) & ~3) <= 64) {
+    obits = (obits + 3) & ~3;
+    sbits = (sbits + 3) & ~3;
+  }
   const int oshift = ibits, sshift = ibits + obits;
   if (sshift + sbits > 64) {
     set_error("ngap_batch_match: stream count, stream length and group count exceed a 64-bit key");
