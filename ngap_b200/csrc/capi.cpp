@@ -219,13 +219,24 @@ int ngap_features_host(const uint8_t* data, uint64_t bytes, const uint64_t* offs
     const double lw = wl ? std::log2((double)wl) : 0.0;
     double sum = 0.0, mx = 0.0;
     for (uint64_t k = 0; k < nwin; k++) {
-      uint32_t c[256] = {0};
+      // four interleaved counters per byte value: a run of equal bytes does
+      // not chain every increment on the previous one
+      uint32_t c4[4][256];
+      std::memset(c4, 0, sizeof(c4));
       const uint8_t* q = p + k * W;
-      for (uint64_t i = 0; i < wl; i++) c[q[i]]++;
+      uint64_t i = 0;
+      for (; i + 4 <= wl; i += 4) {
+        c4[0][q[i]]++;
+        c4[1][q[i + 1]]++;
+        c4[2][q[i + 2]]++;
+        c4[3][q[i + 3]]++;
+      }
+      for (; i < wl; i++) c4[0][q[i]]++;
       double s = 0.0;
       for (int b = 0; b < 256; b++) {
-        s += clogc[c[b]];
-        hist[b] += c[b];
+        const uint32_t cb = c4[0][b] + c4[1][b] + c4[2][b] + c4[3][b];
+        s += clogc[cb];
+        hist[b] += cb;
       }
       const double h = std::max(0.0, lw - s / (double)wl);
       sum += h;
