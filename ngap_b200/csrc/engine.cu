@@ -1127,7 +1127,10 @@ int ngap_match(ngap_engine* e, const ngap_tables* t, const uint8_t* input, int i
   e->sort_chain_pending = 0;
   e->ran = false;
   int algo = p->algorithm;
-  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 1024;
+  // automatic window: 2048 positions (against 1024: Hamming set 0.654 ->
+  // 0.624 ms, high_frontier and the literal set 1-2 % faster; shortened
+  // below when the shared memory of the warps and a staged image does not fit)
+  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 2048;
   int table_depth = 0;
   for (auto& th : t->tiles) table_depth = std::max(table_depth, th.depth);
   switch (algo) {
@@ -1571,7 +1574,10 @@ int ngap_batch_match(ngap_engine* e, const ngap_tableset* ts, const uint8_t* inp
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   e->stream = st;
   e->ran = false;
-  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 1024;
+  // automatic window: 2048 positions (against 1024: Hamming set 0.654 ->
+  // 0.624 ms, high_frontier and the literal set 1-2 % faster; shortened
+  // below when the shared memory of the warps and a staged image does not fit)
+  int depth = 1, priv = 0, window = p->window > 0 ? p->window : 2048;
   int rc = algo_config(p->algorithm, ts->max_depth, &depth, &priv, &window);
   if (rc != NGAP_OK) return rc;
   window = std::min(window, kMaxWindow);
