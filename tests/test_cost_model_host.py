@@ -201,6 +201,11 @@ def test_serving_rejects_requests_that_never_fit():
         else:
             assert r.reports is None
     assert srv.held_bytes() <= srv.budget
+    # host time per request, split by phase, and the loop's slow passes
+    h = m["host_us_per_request"]
+    assert set(h) == {"finish", "predict", "launch", "launch_copy", "launch_match_call"}
+    assert all(v >= 0.0 for v in h.values()) and h["predict"] == 0.0  # no predictor
+    assert len(m["slow_passes"]["longest_ms"]) == min(5, m["slow_passes"]["count"])
 
 
 def test_autotune_search_with_fake_launches():
