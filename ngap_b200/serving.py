@@ -111,28 +111,6 @@ def features_host(datas, window=cm.ENTROPY_WINDOW):
     return out
 
 
-def host_features_many(datas, window=cm.ENTROPY_WINDOW):
-    """host_features of several regions; row i equals host_features(datas[i]).
-    Regions of one common length that is a multiple of `window` (full 16 KiB
-    regions, the usual case) share one histogram pass over all their windows."""
-    out = np.zeros((len(datas), 258), np.float32)
-    full = [i for i, d in enumerate(datas) if len(d) == cm.REGION and cm.REGION % window == 0]
-    for i, d in enumerate(datas):
-        if not full or i not in set(full):
-            out[i] = host_features(d, window)
-    if full:
-        k, nwin = len(full), cm.REGION // window
-        block = np.stack([datas[i] for i in full]).reshape(k * nwin, window)
-        c = np.bincount((_window_base(k * nwin, window) + block.ravel()), minlength=k * nwin * 256)
-        c = c.reshape(k, nwin, 256)
-        q = c / window
-        h = -np.sum(q * np.log2(np.where(q > 0, q, 1.0)), axis=2)  # [k, nwin]
-        out[full, :256] = c.sum(axis=1) / cm.REGION
-        out[full, 256] = h.mean(axis=1) / 8
-        out[full, 257] = h.max(axis=1) / 8
-    return out
-
-
 _bases = {}
 
 
